@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""NL-SAR benchmark: Mpix/s of the fused B200 path on one 4096x4096 InSAR scene.
+
+Workload: the plain NL-SAR configuration on a single 4096 x 4096 float32
+synthetic scene (search window 21, patches {3,5,7}, scales {1,3}, h 15, c 49,
+per-pixel selection by the largest bias-reduced ENL), statistics trained on a
+separate seeded 128 x 128 homogeneous area (reflectivity 1, coherence 0.6).
+Seeded synthetic data stands in for real interferograms.
+
+A step is one full filter of the scene (prep kernels + the fused kernel) with
+inputs resident in HBM (201 MB of inputs, larger than the 126 MB L2, so every
+step streams them from HBM).  `e2e` is the same metric through the public host
+API with pinned host buffers, copies included.  Under torchrun each rank
+filters its own scene (weak scaling, no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NL-SAR Mpix/s"
+UNIT = "Mpix/s"
+SWS, PATCHES, SCALES, H_PARAM, C_PARAM = 21, [3, 5, 7], [1, 3], 15.0, 49.0
+# algorithmic FP32 work per output pixel at these parameters (FMA = 2 flops):
+# pixel similarity 6160 + box sums 5280 + weights 13200 + ENL statistics
+# 29106 + selection 180 + weighted mean 3984 + per-pixel set-up/decompose 46
+FLOP_PER_PIXEL = 57956
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=4096)
+    p.add_argument("--mode", default="argmax_enl", choices=["argmax_enl", "reference"])
+    p.add_argument("--cpu-sample", type=int, default=192, help="side of the CPU-baseline crop")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        finally:
+            os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_stats(dcl, synthetic):
+    t1, t2, tp = synthetic.training_area(128, seed=7)
+    return dcl.nlsar_train_insar(t1, t2, tp, PATCHES, SCALES)
+
+
+def cpu_oracle_rate(a1, a2, ph, stats, side, mode, threads):
+    """The oracle (FP32 restatement of the reference path) on a side x side
+    crop, all host threads: Mpix/s and seconds."""
+    from oracle import pyoracle
+
+    y0 = (a1.shape[0] - side) // 2
+    x0 = (a1.shape[1] - side) // 2
+    crop = [x[y0:y0 + side, x0:x0 + side].copy() for x in (a1, a2, ph)]
+    t = time.perf_counter()
+    pyoracle.nlsar_insar(*crop, SWS, PATCHES, SCALES, stats, H_PARAM, C_PARAM,
+                         select_mode=1 if mode == "argmax_enl" else 0, nthreads=threads)
+    dt = time.perf_counter() - t
+    return side * side / dt / 1e6, dt
+
+
+def traffic_from_profiles(size):
+    """DRAM bytes per fused launch from the committed ncu summary, scaled to
+    `size`, or None."""
+    path = os.path.join(ROOT, "profiles", "nlsar_fused_kernel.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_pixel:"):
+                return float(line.split(":")[1]) * size * size
+    except OSError:
+        pass
+    return None
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+
+    import despeckcl_b200 as dcl  # noqa: F401  (stats container only)
+    from despeckcl_b200 import synthetic
+    from oracle import pyoracle
+
+    threads = os.cpu_count() or 1
+    t1, t2, tp = synthetic.training_area(128, seed=7)
+    stats = pyoracle.training_insar(t1, t2, tp, PATCHES, SCALES)
+    side = min(args.cpu_sample, args.size)
+    a1, a2, ph = synthetic.insar_scene(args.size, args.size, 1)
+    for _ in range(args.warmup):
+        cpu_oracle_rate(a1, a2, ph, stats, min(side, 64), args.mode, threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_oracle_rate(a1, a2, ph, stats, side, args.mode, threads)
+        times.append(dt)
+    ms = 1e3 * sum(times) / len(times)
+    value = side * side / (ms * 1e-3) / 1e6
+    sample = (f"{side}x{side} centre crop of the {args.size}x{args.size} scene per step, FP32 oracle "
+              f"(CPU restatement of the reference path; the OpenCL reference cannot be built here)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"plain NL-SAR, {args.size}x{args.size} scene (CPU sample {side}x{side})",
+                       "search_window": SWS, "patches": PATCHES, "scales": SCALES, "select_mode": args.mode},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import despeckcl_b200 as dcl
+    from despeckcl_b200 import synthetic
+
+    ws, rank, local = dist_env()
+    if ws != args.gpus:
+        args.gpus = ws
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    L = dcl.lib()
+    S = args.size
+    stats = make_stats(dcl, synthetic)
+    a1, a2, ph = synthetic.insar_scene(S, S, 1 + rank)
+    dev = [torch.from_numpy(x).cuda() for x in (a1, a2, ph)]
+    out = tuple(torch.empty((S, S), dtype=torch.float32, device="cuda") for _ in range(3))
+    stream = torch.cuda.current_stream()
+
+    def step():
+        dcl.nlsar_insar_device(*dev, SWS, PATCHES, SCALES, stats, H_PARAM, C_PARAM, select_mode=args.mode, out=out,
+                               stream=stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        L.dcl_profile_begin()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+        fused_ms = ctypes.c_double()
+        fused_n = ctypes.c_long()
+        all_n = ctypes.c_long()
+        rc = L.dcl_profile_end(ctypes.byref(fused_ms), ctypes.byref(fused_n), ctypes.byref(all_n))
+        if rc != 0:
+            raise RuntimeError(L.dcl_last_error().decode())
+    ms_step = start.elapsed_time(stop) / args.steps
+    if dist:
+        t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+    value = args.gpus * S * S / (ms_step * 1e-3) / 1e6
+
+    # end to end through the public host API, pinned host buffers
+    pin = [torch.from_numpy(x).pin_memory() for x in (a1, a2, ph)]
+    hout = [torch.empty((S, S), dtype=torch.float32).pin_memory() for _ in range(3)]
+    hin = [p.numpy() for p in pin]
+    hres = [o.numpy() for o in hout]
+
+    def e2e_step():
+        import despeckcl_b200.api as api
+
+        pk, pp, npn = api._ints(PATCHES)
+        sk, sp, nsn = api._ints(SCALES)
+        arr, n, keep = api._entries(stats)
+        api._check(L.dcl_nlsar_insar(api._fp(hin[0]), api._fp(hin[1]), api._fp(hin[2]), api._fp(hres[0]),
+                                     api._fp(hres[1]), api._fp(hres[2]), S, S, SWS, pp, npn, sp, nsn, arr, n,
+                                     ctypes.c_float(H_PARAM), ctypes.c_float(C_PARAM), api._mode(args.mode)))
+
+    e2e_step()
+    if dist:
+        dist.barrier()
+    ke = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / ke
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = args.gpus * S * S / (e2e_ms * 1e-3) / 1e6
+    np.testing.assert_array_equal(hres[0], out[0].cpu().numpy())  # same result through both entry points
+
+    peak = ctypes.c_double()
+    if L.dcl_measure_fp32_tflops(ctypes.byref(peak)) != 0:
+        raise RuntimeError(L.dcl_last_error().decode())
+    kern_ms = fused_ms.value / max(1, fused_n.value)
+    achieved = FLOP_PER_PIXEL * S * S / (kern_ms * 1e-3) / 1e12
+    traffic = traffic_from_profiles(S)
+
+    cpu = None
+    if rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, dt = cpu_oracle_rate(a1, a2, ph, stats, min(args.cpu_sample, S), args.mode, threads)
+        side = min(args.cpu_sample, S)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{side}x{side} centre crop of the scene, FP32 oracle (CPU restatement of the reference "
+                         f"path), {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, 40 rectangles + fringes, "
+                                                          "single-look speckle)",
+            "config": {"workload": f"plain NL-SAR on one {S}x{S} scene per GPU", "search_window": SWS,
+                       "patches": PATCHES, "scales": SCALES, "h": H_PARAM, "c": C_PARAM,
+                       "select_mode": args.mode, "l2": "inputs 201 MB > L2 126 MB per step",
+                       "parallelism": f"replica x{args.gpus}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * S * S * 4,
+                    "d2h_bytes_per_step": 3 * S * S * 4, "ms_per_step": e2e_ms},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value, "traffic": traffic,
+                         "kernel": "nlsar_fused_kernel", "kernel_ms": kern_ms,
+                         "flop_per_pixel": FLOP_PER_PIXEL,
+                         "peak_source": "measured in-process FP32 FMA probe (dcl_measure_fp32_tflops)"},
+            "gpu_launches": int(all_n.value),
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,150 @@
+// Boxcar InSAR filter: w x w window means of the intensity and of the complex
+// interferogram (src/compute/boxcar/cl_kernels/boxcar_kernel.cl:19-69 in the
+// reference, driven by src/compute/boxcar/boxcar.cpp:30-100 over 512x512 tiles
+// with overlap (w-1)/2).
+//
+// One pass over HBM: each CTA stages its output tile plus a (w-1)/2 halo of
+// (I, Re, Im) = ((a1^2+a2^2)/2, a1 a2 cos phi, a1 a2 sin phi) in shared memory,
+// forms horizontal window sums, then vertical sums, and writes
+// ref = mean I, phase = atan2(Im, Re), coh = |sum Re + j Im| / sum I.
+//
+// Like NL-SAR, the reference's clamped tile write-back puts the result of
+// virtual row H-1+(w-1)/2 of the clamp-extended image into output row H-1
+// (and likewise for the last column); the kernel computes on that virtual
+// plane.
+
+#include <cuda_runtime.h>
+
+#include "../../include/despeckcl_b200.h"
+#include "dcl_internal.h"
+
+namespace dcl {
+namespace {
+
+constexpr int kBoxTW = 64;
+constexpr int kBoxTH = 16;
+constexpr int kBoxThreads = 256;
+constexpr int kBoxMaxR = 15;
+
+__device__ __forceinline__ int clampi_b(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__global__ void __launch_bounds__(kBoxThreads)
+    boxcar_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
+                  float* __restrict__ ref, float* __restrict__ phase, float* __restrict__ coh, int H, int W, int r) {
+  extern __shared__ float sm[];
+  const int SW = kBoxTW + 2 * r, SH = kBoxTH + 2 * r;
+  float* sI = sm;                 // [SH][SW]
+  float* sR = sI + SH * SW;
+  float* sJ = sR + SH * SW;
+  float* hI = sJ + SH * SW;       // [SH][kBoxTW] horizontal sums
+  float* hR = hI + SH * kBoxTW;
+  float* hJ = hR + SH * kBoxTW;
+  const int vy0 = blockIdx.y * kBoxTH, vx0 = blockIdx.x * kBoxTW;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < SH * SW; i += kBoxThreads) {
+    const int rr = i / SW, cc = i - rr * SW;
+    const int y = clampi_b(vy0 - r + rr, 0, H - 1), x = clampi_b(vx0 - r + cc, 0, W - 1);
+    const size_t g = (size_t)y * W + x;
+    const float am = a1[g], as = a2[g];
+    float sn, cs;
+    sincosf(phi[g], &sn, &cs);
+    const float aa = am * as;
+    sI[i] = (am * am + as * as) / 2;
+    sR[i] = aa * cs;
+    sJ[i] = aa * sn;
+  }
+  __syncthreads();
+  for (int i = tid; i < SH * kBoxTW; i += kBoxThreads) {
+    const int rr = i / kBoxTW, cc = i - rr * kBoxTW;
+    const float* pI = sI + rr * SW + cc;
+    const float* pR = sR + rr * SW + cc;
+    const float* pJ = sJ + rr * SW + cc;
+    float si = 0.f, sr = 0.f, sj = 0.f;
+    for (int k = 0; k <= 2 * r; ++k) {
+      si += pI[k];
+      sr += pR[k];
+      sj += pJ[k];
+    }
+    hI[i] = si;
+    hR[i] = sr;
+    hJ[i] = sj;
+  }
+  __syncthreads();
+  const float inv_n = 1.0f / (float)((2 * r + 1) * (2 * r + 1));
+  for (int i = tid; i < kBoxTH * kBoxTW; i += kBoxThreads) {
+    const int rr = i / kBoxTW, cc = i - rr * kBoxTW;
+    const int vy = vy0 + rr, vx = vx0 + cc;
+    const int oy = (vy < H - 1) ? vy : (vy == H - 1 + r ? H - 1 : -1);
+    const int ox = (vx < W - 1) ? vx : (vx == W - 1 + r ? W - 1 : -1);
+    if (oy < 0 || ox < 0) continue;
+    float si = 0.f, sr = 0.f, sj = 0.f;
+    for (int k = 0; k <= 2 * r; ++k) {
+      si += hI[(rr + k) * kBoxTW + cc];
+      sr += hR[(rr + k) * kBoxTW + cc];
+      sj += hJ[(rr + k) * kBoxTW + cc];
+    }
+    const size_t o = (size_t)oy * W + ox;
+    ref[o] = si * inv_n;
+    phase[o] = atan2f(sj, sr);
+    coh[o] = sqrtf(sr * sr + sj * sj) / si;
+  }
+}
+
+}  // namespace
+
+int boxcar_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase, float* coh, int H,
+                  int W, int w, cudaStream_t st) {
+  if (!a1 || !a2 || !phi || !ref || !phase || !coh) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  if (w < 1 || w % 2 == 0 || (w - 1) / 2 > kBoxMaxR)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "window width must be odd and in [1, %d], got %d", 2 * kBoxMaxR + 1, w);
+  const int r = (w - 1) / 2;
+  const int vH = H - 1 + r, vW = W - 1 + r;
+  dim3 grid((vW + kBoxTW) / kBoxTW, (vH + kBoxTH) / kBoxTH);
+  const size_t smem = (size_t)3 * ((kBoxTH + 2 * r) * (kBoxTW + 2 * r) + (kBoxTH + 2 * r) * kBoxTW) * sizeof(float);
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && smem > configured) {
+    cudaError_t e = cudaFuncSetAttribute(boxcar_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(boxcar)");
+    configured = smem;
+  }
+  boxcar_kernel<<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W, r);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "boxcar launch");
+  return DCL_OK;
+}
+
+}  // namespace dcl
+
+extern "C" int dcl_boxcar_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+                                 float* coh, int H, int W, int window_width, void* stream) {
+  return dcl::boxcar_device(a1, a2, phi, ref, phase, coh, H, W, window_width, (cudaStream_t)stream);
+}
+
+extern "C" int dcl_boxcar(const float* a1, const float* a2, const float* phi, float* ref, float* phase, float* coh,
+                          int H, int W, int window_width) {
+  if (!a1 || !a2 || !phi || !ref || !phase || !coh) return dcl::set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return dcl::set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  cudaStream_t st = cudaStreamPerThread;
+  const size_t n = (size_t)H * W, b = n * sizeof(float);
+  float* buf = nullptr;
+  cudaError_t e = cudaMallocAsync(&buf, 6 * b, st);
+  if (e != cudaSuccess) return dcl::cuda_error(e, "cudaMallocAsync(boxcar)");
+  e = cudaMemcpyAsync(buf, a1, b, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n, a2, b, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 2 * n, phi, b, cudaMemcpyHostToDevice, st);
+  int rc = DCL_OK;
+  if (e != cudaSuccess) rc = dcl::cuda_error(e, "cudaMemcpyAsync(H2D)");
+  if (rc == DCL_OK) rc = dcl::boxcar_device(buf, buf + n, buf + 2 * n, buf + 3 * n, buf + 4 * n, buf + 5 * n, H, W,
+                                            window_width, st);
+  if (rc == DCL_OK) {
+    e = cudaMemcpyAsync(ref, buf + 3 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(phase, buf + 4 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(coh, buf + 5 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = dcl::cuda_error(e, "cudaMemcpyAsync(D2H)");
+  }
+  cudaFreeAsync(buf, st);
+  e = cudaStreamSynchronize(st);
+  if (rc == DCL_OK && e != cudaSuccess) rc = dcl::cuda_error(e, "boxcar");
+  return rc;
+}

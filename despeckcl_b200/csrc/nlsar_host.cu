@@ -1,0 +1,638 @@
+// Host orchestration of the fused NL-SAR engine and its C ABI.
+//
+// Mirrors the reference's driver (src/compute/nlsar/nlsar.cpp:81-194) and
+// per-tile pipeline (src/compute/nlsar/nlsar_filter_sub_image.cpp:146-390)
+// without tiles on the host: arguments are validated, the (patch, scale)
+// combinations are ordered as the reference orders them, the LUTs are folded
+// into one composite weight table per combination, the scene is expanded once
+// into its clamp-padded virtual plane, and one fused launch filters every tile.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/despeckcl_b200.h"
+#include "dcl_internal.h"
+#include "nlsar_common.cuh"
+
+namespace dcl {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char* where) {
+  if (e == cudaErrorMemoryAllocation) return set_error(DCL_ERR_OUT_OF_MEMORY, "%s: %s", where, cudaGetErrorString(e));
+  return set_error(DCL_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+const char* last_error() { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------------------
+// plan: validated parameters -> FilterParams
+// ---------------------------------------------------------------------------
+
+std::vector<float> gauss_weights(int s) {
+  // cl_wrappers/covmat_spatial_avg.cpp:35-50 (exponent in double, float storage,
+  // float normalisation sum)
+  std::vector<float> g;
+  const int ssh = (s - 1) / 2;
+  for (int x = -ssh; x <= ssh; ++x)
+    for (int y = -ssh; y <= ssh; ++y) {
+      const double den = std::pow((double)((float)ssh + 0.5f), 2.0);
+      g.push_back((float)std::exp(-M_PI * (x * x + y * y) / den));
+    }
+  float K = 0.0f;
+  for (float e : g) K += e;
+  for (float& e : g) e = e / K;
+  return g;
+}
+
+float rescale_gamma_2x2() {
+  // covmat_rescale.cl:25-26 with nlooks = 1, dimension = 2
+  return std::pow(std::min(1.0f / 2.0f, 1.0f), 0.33333f);
+}
+
+struct Plan {
+  FilterParams P;
+  std::vector<float> wtab;
+  std::vector<int> scales;       // distinct scale sizes, caller order (scale slots)
+  std::vector<char> slot_used;   // slots referenced by the passes
+  int overlap = 0;
+  int shm = 0;                   // largest scale half among used slots
+  bool full8 = false;
+  int px = 4;
+};
+
+static int validate_sizes(int sws, const int* patches, int np, const int* scales, int ns, std::vector<int>& P,
+                          std::vector<int>& S) {
+  if (sws < 1 || sws % 2 == 0 || sws > kMaxSws)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "search_window_size must be odd and in [1, %d], got %d", kMaxSws, sws);
+  if (!patches || np < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "patch_sizes must not be empty");
+  if (!scales || ns < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "scale_sizes must not be empty");
+  P.clear();
+  S.clear();
+  for (int i = 0; i < np; ++i) {
+    const int p = patches[i];
+    if (p < 1 || p % 2 == 0 || p > 2 * kMaxPatchHalf + 1)
+      return set_error(DCL_ERR_INVALID_ARGUMENT, "patch sizes must be odd and in [1, %d], got %d",
+                       2 * kMaxPatchHalf + 1, p);
+    if (std::find(P.begin(), P.end(), p) == P.end()) P.push_back(p);
+  }
+  for (int i = 0; i < ns; ++i) {
+    const int s = scales[i];
+    if (s < 1 || s % 2 == 0 || s * s > kMaxGauss)
+      return set_error(DCL_ERR_INVALID_ARGUMENT, "scale sizes must be odd and in [1, 9], got %d", s);
+    if (std::find(S.begin(), S.end(), s) == S.end()) S.push_back(s);
+  }
+  if ((int)S.size() > kMaxScales) return set_error(DCL_ERR_INVALID_ARGUMENT, "at most %d scale sizes", kMaxScales);
+  if ((int)(P.size() * S.size()) > kMaxCombos)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "at most %d (patch, scale) combinations", kMaxCombos);
+  return DCL_OK;
+}
+
+int make_plan(int sws, const int* patches, int np, const int* scales, int ns, const dcl_stats_entry* stats,
+              int nstats, float h, float c, int select_mode, bool full8, Plan& pl) {
+  std::vector<int> Pv, Sv;
+  int rc = validate_sizes(sws, patches, np, scales, ns, Pv, Sv);
+  if (rc) return rc;
+  if (!stats || nstats < 1) return set_error(DCL_ERR_MISSING_STATS, "no NL-SAR statistics given");
+  if (select_mode != DCL_SELECT_REFERENCE && select_mode != DCL_SELECT_ARGMAX_ENL)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "unknown select_mode %d", select_mode);
+  if (!(h > 0.0f) || !std::isfinite(h)) return set_error(DCL_ERR_INVALID_ARGUMENT, "h_param must be > 0");
+  if (!std::isfinite(c)) return set_error(DCL_ERR_INVALID_ARGUMENT, "c_param must be finite");
+  // the statistics map, keyed and ordered like std::map<nlsar::params, ...>
+  // (parameters.h:37-40: lexicographic (patch, scale))
+  std::map<std::pair<int, int>, const dcl_stats_entry*> smap;
+  for (int i = 0; i < nstats; ++i) {
+    const dcl_stats_entry& e = stats[i];
+    if (e.lut_size < 2 || e.lut_size > (unsigned)kMaxLut || !e.quantilles || !e.chi2cdf_inv)
+      return set_error(DCL_ERR_INVALID_ARGUMENT, "stats (%d,%d): lut_size must be in [2, %d] with both tables",
+                       e.patch_size, e.scale_size, kMaxLut);
+    if (!(e.dissims_max > e.dissims_min))
+      return set_error(DCL_ERR_INVALID_ARGUMENT, "stats (%d,%d): dissims_max must exceed dissims_min", e.patch_size,
+                       e.scale_size);
+    smap[{e.patch_size, e.scale_size}] = &e;
+  }
+  std::map<std::pair<int, int>, int> rank;
+  {
+    int r = 0;
+    for (auto& kv : smap) rank[kv.first] = r++;
+  }
+  for (int s : Sv)
+    for (int p : Pv)
+      if (!smap.count({p, s}))
+        return set_error(DCL_ERR_MISSING_STATS, "no statistics for patch size %d, scale size %d", p, s);
+
+  FilterParams& F = pl.P;
+  std::memset(&F, 0, sizeof F);
+  pl.full8 = full8;
+  pl.px = full8 ? 2 : 4;
+  pl.scales = Sv;
+  pl.slot_used.assign(Sv.size(), 0);
+  F.sws = sws;
+  F.wsh = (sws - 1) / 2;
+  F.n_off = sws * sws - 1;
+  F.select_mode = select_mode == DCL_SELECT_ARGMAX_ENL ? 1 : 0;
+  F.c2d = 2 * 2 * std::log(2.0f);
+  F.fallback_combo = 0;
+  F.tile_h = kWarps * pl.px;
+  const int pmax = *std::max_element(Pv.begin(), Pv.end());
+  const int smax = *std::max_element(Sv.begin(), Sv.end());
+  pl.overlap = (pmax - 1) / 2 + F.wsh + (smax - 1) / 2;  // nlsar.cpp:41-51
+
+  // combinations in the reference loop order (nlsar_filter_sub_image.cpp:449-470)
+  struct C { int p, s, slot; };
+  std::vector<C> combos;
+  for (size_t si = 0; si < Sv.size(); ++si)
+    for (int p : Pv) combos.push_back({p, Sv[si], (int)si});
+  F.ncombo = (int)combos.size();
+  pl.wtab.assign((size_t)F.ncombo * kMaxLut, 0.0f);
+  for (int ci = 0; ci < F.ncombo; ++ci) {
+    const dcl_stats_entry& e = *smap[{combos[ci].p, combos[ci].s}];
+    ComboParams& cp = F.combo[ci];
+    cp.dmin = e.dissims_min;
+    cp.dmax = e.dissims_max;
+    cp.span = e.dissims_max - e.dissims_min;
+    cp.lm1 = (float)(int)(e.lut_size - 1);
+    cp.rank = rank[{combos[ci].p, combos[ci].s}];
+    // compute_weights.cl:49-51 folded into one table indexed by the first LUT index
+    for (unsigned k = 0; k < e.lut_size; ++k) {
+      const float q = e.quantilles[k];
+      float qi = q * (float)(int)(e.lut_size - 1);
+      unsigned i2 = (qi > 0.0f) ? (unsigned)qi : 0u;
+      if (i2 >= e.lut_size) i2 = e.lut_size - 1;
+      const float x = e.chi2cdf_inv[i2];
+      pl.wtab[(size_t)ci * kMaxLut + k] = std::exp(-std::fabs(x - c) / h);
+    }
+  }
+
+  // passes
+  auto add_pass = [&](int slot, std::vector<int> ps) {
+    std::sort(ps.begin(), ps.end());
+    for (size_t g = 0; g < ps.size(); g += kPatchPerPass) {
+      if (F.npass >= kMaxPasses) return false;
+      PassParams& pp = F.pass[F.npass++];
+      pp.scale_slot = slot;
+      pp.np = (int)std::min<size_t>(kPatchPerPass, ps.size() - g);
+      for (int j = 0; j < pp.np; ++j) {
+        const int p = ps[g + j];
+        pp.ph[j] = (p - 1) / 2;
+        for (int ci = 0; ci < F.ncombo; ++ci)
+          if (combos[ci].p == p && combos[ci].slot == slot) pp.combo[j] = ci;
+      }
+      pl.slot_used[slot] = 1;
+    }
+    return true;
+  };
+  if (F.select_mode == 1) {
+    for (size_t si = 0; si < Sv.size(); ++si)
+      if (!add_pass((int)si, Pv)) return set_error(DCL_ERR_INVALID_ARGUMENT, "too many (scale, patch) passes");
+  } else {
+    // best_params.cpp:27-54: every pixel takes the last key of the map.  A key
+    // outside patch_sizes x scale_sizes maps to index 0 of the loop order
+    // (params2idx default) with the zero-initialised alpha
+    // (nlsar_filter_sub_image.cpp:418-422, 541, 545)
+    const std::pair<int, int> last = smap.rbegin()->first;
+    int ci_last = -1;
+    for (int ci = 0; ci < F.ncombo; ++ci)
+      if (combos[ci].p == last.first && combos[ci].s == last.second) ci_last = ci;
+    if (ci_last < 0) {
+      ci_last = 0;
+      F.alpha_zero = 1;
+    }
+    add_pass(combos[ci_last].slot, {combos[ci_last].p});
+  }
+  F.phm = 0;
+  for (int i = 0; i < F.npass; ++i)
+    for (int j = 0; j < F.pass[i].np; ++j) F.phm = std::max(F.phm, F.pass[i].ph[j]);
+  pl.shm = 0;
+  for (size_t si = 0; si < Sv.size(); ++si)
+    if (pl.slot_used[si]) pl.shm = std::max(pl.shm, (Sv[si] - 1) / 2);
+  F.G = F.wsh + F.phm + pl.shm;
+  return DCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device state
+// ---------------------------------------------------------------------------
+
+static std::mutex g_init_mu;
+static bool g_pool_ready[64];
+
+static int ensure_device_ready(int& dev) {
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (dev >= 0 && dev < 64 && !g_pool_ready[dev]) {
+    // keep freed scratch in the stream-ordered pool between calls
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    g_pool_ready[dev] = true;
+  }
+  return DCL_OK;
+}
+
+int choose_k(const Plan& pl, size_t& smem_bytes) {
+  int optin = 0, dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || optin <= 0)
+    optin = 227 * 1024;
+  for (int K = 8; K >= 1; --K) {
+    const SmemLayout L = smem_layout(pl.P.tile_h, pl.P.wsh, pl.P.phm, K, pl.full8);
+    const size_t b = (size_t)L.total * 4;
+    if (b <= (size_t)optin) {
+      smem_bytes = b;
+      return K;
+    }
+  }
+  return 0;
+}
+
+// Geometry of one scene on the virtual plane.
+struct SceneGeom {
+  int H, W, vH, vW, tiles_x, tiles_y, Hp, Wp, pitch;
+};
+
+SceneGeom scene_geom(const Plan& pl, int H, int W) {
+  SceneGeom g;
+  g.H = H;
+  g.W = W;
+  g.vH = H - 1 + pl.overlap;
+  g.vW = W - 1 + pl.overlap;
+  g.tiles_y = (g.vH + 1 + pl.P.tile_h - 1) / pl.P.tile_h;
+  g.tiles_x = (g.vW + 1 + kTileW - 1) / kTileW;
+  g.Hp = g.tiles_y * pl.P.tile_h + 2 * pl.P.G;
+  g.Wp = g.tiles_x * kTileW + 2 * pl.P.G;
+  g.pitch = (g.Wp + 7) / 8 * 8;
+  return g;
+}
+
+size_t scratch_bytes(const Plan& pl, const SceneGeom& g) {
+  const size_t plane = (size_t)g.Hp * g.pitch;
+  size_t b = plane * sizeof(float4) * (pl.full8 ? 2 : 1);
+  for (size_t si = 0; si < pl.scales.size(); ++si)
+    if (pl.slot_used[si]) b += plane * (sizeof(float4) + sizeof(float));
+  return b;
+}
+
+// Carve the scratch of one scene and fill its descriptor (pointers into `base`).
+void carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d) {
+  const size_t plane = (size_t)g.Hp * g.pitch;
+  char* p = base;
+  d.cori = reinterpret_cast<float4*>(p);
+  p += plane * sizeof(float4);
+  d.cori2 = nullptr;
+  if (pl.full8) {
+    d.cori2 = reinterpret_cast<float4*>(p);
+    p += plane * sizeof(float4);
+  }
+  for (int si = 0; si < kMaxScales; ++si) {
+    d.cs[si] = nullptr;
+    d.ld[si] = nullptr;
+  }
+  for (size_t si = 0; si < pl.scales.size(); ++si)
+    if (pl.slot_used[si]) {
+      d.cs[si] = reinterpret_cast<float4*>(p);
+      p += plane * sizeof(float4);
+      d.ld[si] = reinterpret_cast<float*>(p);
+      p += plane * sizeof(float);
+    }
+  d.H = g.H;
+  d.W = g.W;
+  d.vH = g.vH;
+  d.vW = g.vW;
+  d.pitch = g.pitch;
+  d.tiles_x = g.tiles_x;
+  d.tiles_y = g.tiles_y;
+}
+
+// Optional timing of the fused kernel (dcl_profile_begin / dcl_profile_end):
+// CUDA events recorded on the launching stream around every fused launch of
+// the calling thread.
+struct ProfileState {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  long launches = 0;  // all kernels launched by the library while profiling
+};
+static thread_local ProfileState g_prof;
+
+void profile_count(int n) {
+  if (g_prof.on) g_prof.launches += n;
+}
+
+int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
+                const float* phi, const float* cov_in, cudaStream_t st) {
+  dim3 blk(32, 8), grd((g.Wp + 31) / 32, (g.Hp + 7) / 8);
+  int used = 0;
+  for (char u : pl.slot_used) used += u ? 1 : 0;
+  profile_count(1 + used);
+  if (pl.full8)
+    prep_cov_planes_kernel<<<grd, blk, 0, st>>>(cov_in, g.H, g.W, const_cast<float4*>(d.cori),
+                                                const_cast<float4*>(d.cori2), g.Hp, g.Wp, g.pitch, pl.P.G);
+  else
+    prep_cov_insar_kernel<<<grd, blk, 0, st>>>(a1, a2, phi, g.H, g.W, const_cast<float4*>(d.cori), g.Hp, g.Wp,
+                                               g.pitch, pl.P.G);
+  const float gamma = rescale_gamma_2x2();
+  for (size_t si = 0; si < pl.scales.size(); ++si) {
+    if (!pl.slot_used[si]) continue;
+    GaussArg ga;
+    std::memset(&ga, 0, sizeof ga);
+    const std::vector<float> gw = gauss_weights(pl.scales[si]);
+    std::copy(gw.begin(), gw.end(), ga.g);
+    prep_scale_kernel<<<grd, blk, 0, st>>>(d.cori, g.Hp, g.Wp, g.pitch, pl.scales[si], ga, gamma,
+                                           const_cast<float4*>(d.cs[si]), const_cast<float*>(d.ld[si]));
+  }
+  return DCL_OK;
+}
+
+int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (g_prof.on) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+  }
+  const cudaError_t e = launch_nlsar_fused(pl.full8, F, d_scenes, smem, F.total_tiles, st);
+  if (g_prof.on) {
+    cudaEventRecord(b, st);
+    g_prof.ev.push_back({a, b});
+    g_prof.launches += 1;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "NL-SAR fused launch");
+  return DCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one call on device pointers (single scene or batch)
+// ---------------------------------------------------------------------------
+
+struct SceneIO {
+  const float *a1, *a2, *phi, *cov_in;
+  float *ref, *phase, *coh, *cov_out;
+  int* sel;
+  int H, W;
+};
+
+int run_device(const Plan& pl0, const std::vector<SceneIO>& io, cudaStream_t st) {
+  int dev;
+  int rc = ensure_device_ready(dev);
+  if (rc) return rc;
+  Plan pl = pl0;
+  size_t smem = 0;
+  const int K = choose_k(pl, smem);
+  if (K < 1) return set_error(DCL_ERR_UNSUPPORTED, "search window / patch sizes too large for shared memory");
+  pl.P.K = K;
+
+  std::vector<SceneGeom> geo;
+  std::vector<size_t> offs;
+  size_t total = 0;
+  int tiles = 0;
+  for (const SceneIO& s : io) {
+    if (s.H < 1 || s.W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+    geo.push_back(scene_geom(pl, s.H, s.W));
+    offs.push_back(total);
+    total += (scratch_bytes(pl, geo.back()) + 255) / 256 * 256;
+    const long long t = (long long)geo.back().tiles_x * geo.back().tiles_y;
+    if (t + tiles > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
+    tiles += (int)t;
+  }
+  const size_t desc_bytes = io.size() * sizeof(SceneDesc);
+  const size_t wtab_bytes = pl.wtab.size() * sizeof(float);
+  char* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, total + desc_bytes + wtab_bytes + 512, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(scratch)");
+  SceneDesc* d_desc = reinterpret_cast<SceneDesc*>(scratch + (total + 255) / 256 * 256);
+  float* d_wtab = reinterpret_cast<float*>(reinterpret_cast<char*>(d_desc) + (desc_bytes + 255) / 256 * 256);
+
+  std::vector<SceneDesc> desc(io.size());
+  int tb = 0;
+  for (size_t i = 0; i < io.size(); ++i) {
+    std::memset(&desc[i], 0, sizeof(SceneDesc));
+    carve_scene(pl, geo[i], scratch + offs[i], desc[i]);
+    desc[i].ref = io[i].ref;
+    desc[i].phase = io[i].phase;
+    desc[i].coh = io[i].coh;
+    desc[i].cov_out = io[i].cov_out;
+    desc[i].sel_out = io[i].sel;
+    desc[i].tile_begin = tb;
+    tb += geo[i].tiles_x * geo[i].tiles_y;
+    launch_prep(pl, geo[i], desc[i], io[i].a1, io[i].a2, io[i].phi, io[i].cov_in, st);
+  }
+  e = cudaMemcpyAsync(d_desc, desc.data(), desc_bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_wtab, pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(scratch, st);
+    return cuda_error(e, "cudaMemcpyAsync(params)");
+  }
+  pl.P.wtab = d_wtab;
+  pl.P.n_scenes = (int)io.size();
+  pl.P.total_tiles = tiles;
+  rc = launch_fused(pl, pl.P, d_desc, smem, st);
+  e = cudaGetLastError();
+  cudaFreeAsync(scratch, st);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_error(e, "NL-SAR launch");
+  // the host vectors above were staged by cudaMemcpyAsync (pageable source),
+  // so they may go out of scope now
+  return DCL_OK;
+}
+
+// host pointers: copy in, run, copy out (the reference's filter_sub_image
+// uploads and downloads the same way, nlsar/conversion.cpp:22-142)
+int run_host_insar(const Plan& pl, const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+                   float* coh, int H, int W) {
+  if (!a1 || !a2 || !phi || !ref || !phase || !coh) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  int dev;
+  int rc = ensure_device_ready(dev);
+  if (rc) return rc;
+  cudaStream_t st = cudaStreamPerThread;
+  const size_t n = (size_t)H * W, b = n * sizeof(float);
+  float* buf = nullptr;
+  cudaError_t e = cudaMallocAsync(&buf, 6 * b, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io)");
+  e = cudaMemcpyAsync(buf, a1, b, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n, a2, b, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 2 * n, phi, b, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(buf, st);
+    return cuda_error(e, "cudaMemcpyAsync(H2D)");
+  }
+  SceneIO s{buf, buf + n, buf + 2 * n, nullptr, buf + 3 * n, buf + 4 * n, buf + 5 * n, nullptr, nullptr, H, W};
+  rc = run_device(pl, {s}, st);
+  if (rc == DCL_OK) {
+    e = cudaMemcpyAsync(ref, buf + 3 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(phase, buf + 4 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(coh, buf + 5 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
+  }
+  cudaFreeAsync(buf, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR");
+  return rc;
+}
+
+int run_host_covmat(const Plan& pl, const float* cin, float* cout, int H, int W) {
+  if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  int dev;
+  int rc = ensure_device_ready(dev);
+  if (rc) return rc;
+  cudaStream_t st = cudaStreamPerThread;
+  const size_t n = (size_t)8 * H * W, b = n * sizeof(float);
+  float* buf = nullptr;
+  cudaError_t e = cudaMallocAsync(&buf, 2 * b, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io)");
+  e = cudaMemcpyAsync(buf, cin, b, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(buf, st);
+    return cuda_error(e, "cudaMemcpyAsync(H2D)");
+  }
+  SceneIO s{nullptr, nullptr, nullptr, buf, nullptr, nullptr, nullptr, buf + n, nullptr, H, W};
+  rc = run_device(pl, {s}, st);
+  if (rc == DCL_OK) {
+    e = cudaMemcpyAsync(cout, buf + n, b, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
+  }
+  cudaFreeAsync(buf, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR");
+  return rc;
+}
+
+}  // namespace dcl
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+using namespace dcl;
+
+extern "C" const char* dcl_last_error(void) { return last_error(); }
+
+extern "C" const char* dcl_version(void) { return "despeckcl_b200 0.1 (sm_100a)"; }
+
+extern "C" void dcl_profile_begin(void) {
+  for (auto& p : g_prof.ev) {
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  g_prof.ev.clear();
+  g_prof.launches = 0;
+  g_prof.on = true;
+}
+
+extern "C" int dcl_profile_end(double* fused_ms, long* fused_launches, long* all_launches) {
+  double total = 0.0;
+  int rc = DCL_OK;
+  for (auto& p : g_prof.ev) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventSynchronize(p.second);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, p.first, p.second);
+    if (e != cudaSuccess && rc == DCL_OK) rc = cuda_error(e, "profile events");
+    total += ms;
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  if (fused_ms) *fused_ms = total;
+  if (fused_launches) *fused_launches = (long)g_prof.ev.size();
+  if (all_launches) *all_launches = g_prof.launches;
+  g_prof.ev.clear();
+  g_prof.launches = 0;
+  g_prof.on = false;
+  return rc;
+}
+
+extern "C" int dcl_nlsar_insar(const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+                               float* coh, int H, int W, int sws, const int* patches, int np, const int* scales,
+                               int ns, const dcl_stats_entry* stats, int nstats, float h, float c, int select_mode) {
+  Plan pl;
+  int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, false, pl);
+  if (rc) return rc;
+  return run_host_insar(pl, a1, a2, phi, ref, phase, coh, H, W);
+}
+
+extern "C" int dcl_nlsar_insar_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+                                      float* coh, int H, int W, int sws, const int* patches, int np,
+                                      const int* scales, int ns, const dcl_stats_entry* stats, int nstats, float h,
+                                      float c, int select_mode, int* selection_out, void* stream) {
+  if (!a1 || !a2 || !phi || !ref || !phase || !coh) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  Plan pl;
+  int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, false, pl);
+  if (rc) return rc;
+  SceneIO s{a1, a2, phi, nullptr, ref, phase, coh, nullptr, selection_out, H, W};
+  return run_device(pl, {s}, (cudaStream_t)stream);
+}
+
+extern "C" int dcl_nlsar_covmat(const float* cin, float* cout, int H, int W, int dim, int sws, const int* patches,
+                                int np, const int* scales, int ns, const dcl_stats_entry* stats, int nstats, float h,
+                                float c, int select_mode) {
+  if (dim != 2)
+    return set_error(dim == 3 ? DCL_ERR_UNSUPPORTED : DCL_ERR_INVALID_ARGUMENT,
+                     "covariance dimension %d: only 2x2 (InSAR) covariances are supported", dim);
+  Plan pl;
+  int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, true, pl);
+  if (rc) return rc;
+  return run_host_covmat(pl, cin, cout, H, W);
+}
+
+extern "C" int dcl_nlsar_covmat_device(const float* cin, float* cout, int H, int W, int dim, int sws,
+                                       const int* patches, int np, const int* scales, int ns,
+                                       const dcl_stats_entry* stats, int nstats, float h, float c, int select_mode,
+                                       void* stream) {
+  if (dim != 2)
+    return set_error(dim == 3 ? DCL_ERR_UNSUPPORTED : DCL_ERR_INVALID_ARGUMENT,
+                     "covariance dimension %d: only 2x2 (InSAR) covariances are supported", dim);
+  if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  Plan pl;
+  int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, true, pl);
+  if (rc) return rc;
+  SceneIO s{nullptr, nullptr, nullptr, cin, nullptr, nullptr, nullptr, cout, nullptr, H, W};
+  return run_device(pl, {s}, (cudaStream_t)stream);
+}
+
+extern "C" int dcl_nlsar_insar_batch_device(int n, const float* const* a1, const float* const* a2,
+                                            const float* const* phi, float* const* ref, float* const* phase,
+                                            float* const* coh, const int* heights, const int* widths, int sws,
+                                            const int* patches, int np, const int* scales, int ns,
+                                            const dcl_stats_entry* stats, int nstats, float h, float c,
+                                            int select_mode, void* stream) {
+  if (n < 1 || !a1 || !a2 || !phi || !ref || !phase || !coh || !heights || !widths)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "empty batch or null pointer");
+  Plan pl;
+  int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, false, pl);
+  if (rc) return rc;
+  std::vector<SceneIO> io;
+  for (int i = 0; i < n; ++i) {
+    if (!a1[i] || !a2[i] || !phi[i] || !ref[i] || !phase[i] || !coh[i])
+      return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer in scene %d", i);
+    io.push_back(SceneIO{a1[i], a2[i], phi[i], nullptr, ref[i], phase[i], coh[i], nullptr, nullptr, heights[i],
+                         widths[i]});
+  }
+  return run_device(pl, io, (cudaStream_t)stream);
+}

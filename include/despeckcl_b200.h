@@ -1,0 +1,168 @@
+/* despeckcl_b200: C ABI of the B200-native NL-SAR engine.
+ *
+ * Plain pointers and sizes only.  Every entry point returns 0 on success and a
+ * negative dcl_status on failure; dcl_last_error() describes the last failure
+ * of the calling thread.  Host-pointer entry points copy inputs to the GPU and
+ * results back, like the reference's filter drivers; *_device entry points
+ * take device pointers and a cudaStream_t (passed as void*) and do not
+ * synchronise.
+ *
+ * Reference interfaces replaced (paths relative to the despeckCL project root):
+ *   dcl_nlsar_insar*         despeckcl::nlsar(float* ampl_master, ...)   include/despeckcl.h:45-59,
+ *                                                                          src/compute/nlsar/nlsar.cpp:139-167
+ *   dcl_nlsar_covmat*        despeckcl::nlsar(float* covmat_raw, ...)    include/despeckcl.h:62-73,
+ *                                                                          src/compute/nlsar/nlsar.cpp:171-194
+ *   dcl_nlsar_training_*     despeckcl::nlsar_training(...)              include/despeckcl.h:75-92,
+ *                                                                          src/compute/nlsar/training/nlsar_training.cpp:57-96
+ *   dcl_stats_save/load      despeckcl::store/load_nlsar_stats_collection include/despeckcl.h:94-95,
+ *                                                                          src/compute/nlsar/training/nlsar_training.cpp:99-113
+ *   dcl_boxcar*              despeckcl::boxcar(...)                      include/despeckcl.h:34-43,
+ *                                                                          src/compute/boxcar/boxcar.cpp:30-100
+ *   dcl_stats_entry          nlsar::params + nlsar::stats                include/compute/nlsar/parameters.h:26-57,
+ *                                                                          include/compute/nlsar/stats.h:28-55
+ */
+#ifndef DESPECKCL_B200_H
+#define DESPECKCL_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dcl_status {
+  DCL_OK = 0,
+  DCL_ERR_INVALID_ARGUMENT = -1,
+  DCL_ERR_MISSING_STATS = -2,
+  DCL_ERR_OUT_OF_MEMORY = -3,
+  DCL_ERR_CUDA = -4,
+  DCL_ERR_UNSUPPORTED = -5,
+  DCL_ERR_TIMEOUT = -6,
+  DCL_ERR_IO = -7
+};
+
+/* Per-pixel (patch, scale) selection.
+ * DCL_SELECT_REFERENCE reproduces nlsar::get_best_params
+ * (src/compute/nlsar/best_params.cpp:27-54): every pixel takes the last key of
+ * the statistics map in (patch, scale) order.
+ * DCL_SELECT_ARGMAX_ENL takes, per pixel, the combination with the largest
+ * bias-reduced ENL (first in map order on ties), the documented NL-SAR rule. */
+enum dcl_select_mode { DCL_SELECT_REFERENCE = 0, DCL_SELECT_ARGMAX_ENL = 1 };
+
+/* One entry of an NL-SAR statistics collection: the key nlsar::params and the
+ * fields of nlsar::stats.  quantilles and chi2cdf_inv hold lut_size floats. */
+typedef struct dcl_stats_entry {
+  int patch_size;
+  int scale_size;
+  unsigned int lut_size;
+  float dissims_min;
+  float dissims_max;
+  const float* quantilles;
+  const float* chi2cdf_inv;
+} dcl_stats_entry;
+
+/* Opaque statistics collection owned by the library (training and loading). */
+typedef struct dcl_stats_collection dcl_stats_collection;
+
+const char* dcl_last_error(void);
+const char* dcl_version(void);
+
+/* Timing of this library's kernels on the calling thread (no reference
+ * counterpart; the reference's timed_run, src/clcfg/clcfg.h:97-119, measures
+ * host wall clock).  Between begin and end, CUDA events are recorded on the
+ * launching stream around every fused NL-SAR launch; end waits for them and
+ * returns the summed fused-kernel time, the number of fused launches and the
+ * number of all kernels the library launched. */
+void dcl_profile_begin(void);
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (FMA = 2
+ * flops): the roofline denominator for the fused NL-SAR kernel.  No
+ * reference counterpart. */
+int dcl_measure_fp32_tflops(double* tflops);
+int dcl_profile_end(double* fused_ms, long* fused_launches, long* all_launches);
+
+/* NL-SAR on an InSAR pair; host pointers, row-major height x width float32.
+ * Replaces despeckcl::nlsar (include/despeckcl.h:45-59). */
+int dcl_nlsar_insar(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                    float* phase_filt, float* coh_filt, int height, int width, int search_window_size,
+                    const int* patch_sizes, int n_patch_sizes, const int* scale_sizes, int n_scale_sizes,
+                    const dcl_stats_entry* stats, int n_stats, float h_param, float c_param, int select_mode);
+
+/* Same on device pointers, asynchronous on `stream`.  selection_out (device,
+ * height x width int32, may be NULL) receives the selected combination's index
+ * in the reference loop order (scale outer, patch inner).  Replaces
+ * despeckcl::nlsar (include/despeckcl.h:45-59). */
+int dcl_nlsar_insar_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                           float* phase_filt, float* coh_filt, int height, int width, int search_window_size,
+                           const int* patch_sizes, int n_patch_sizes, const int* scale_sizes, int n_scale_sizes,
+                           const dcl_stats_entry* stats, int n_stats, float h_param, float c_param,
+                           int select_mode, int* selection_out, void* stream);
+
+/* NL-SAR on a covariance image [2*dim*dim][height][width] (even planes real,
+ * odd planes imaginary), host pointers.  dim 2 only (dim 3 returns
+ * DCL_ERR_UNSUPPORTED).  Replaces despeckcl::nlsar (include/despeckcl.h:62-73). */
+int dcl_nlsar_covmat(const float* covmat_raw, float* covmat_filt, int height, int width, int dim,
+                     int search_window_size, const int* patch_sizes, int n_patch_sizes, const int* scale_sizes,
+                     int n_scale_sizes, const dcl_stats_entry* stats, int n_stats, float h_param, float c_param,
+                     int select_mode);
+
+/* Same on device pointers.  Replaces despeckcl::nlsar (include/despeckcl.h:62-73). */
+int dcl_nlsar_covmat_device(const float* covmat_raw, float* covmat_filt, int height, int width, int dim,
+                            int search_window_size, const int* patch_sizes, int n_patch_sizes,
+                            const int* scale_sizes, int n_scale_sizes, const dcl_stats_entry* stats, int n_stats,
+                            float h_param, float c_param, int select_mode, void* stream);
+
+/* Batched NL-SAR: n_scenes InSAR pairs of possibly different sizes, all
+ * filtered with the same parameters in one persistent launch.  Each array
+ * holds n_scenes device pointers / sizes.  The batched counterpart of
+ * despeckcl::nlsar (include/despeckcl.h:45-59). */
+int dcl_nlsar_insar_batch_device(int n_scenes, const float* const* ampl_master, const float* const* ampl_slave,
+                                 const float* const* phase, float* const* ref_filt, float* const* phase_filt,
+                                 float* const* coh_filt, const int* heights, const int* widths,
+                                 int search_window_size, const int* patch_sizes, int n_patch_sizes,
+                                 const int* scale_sizes, int n_scale_sizes, const dcl_stats_entry* stats,
+                                 int n_stats, float h_param, float c_param, int select_mode, void* stream);
+
+/* Boxcar filter with a window_width x window_width window; host pointers.
+ * Replaces despeckcl::boxcar (include/despeckcl.h:34-43). */
+int dcl_boxcar(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+               float* phase_filt, float* coh_filt, int height, int width, int window_width);
+
+/* Same on device pointers, asynchronous on `stream`.  Replaces
+ * despeckcl::boxcar (include/despeckcl.h:34-43). */
+int dcl_boxcar_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                      float* phase_filt, float* coh_filt, int height, int width, int window_width, void* stream);
+
+/* Training on a homogeneous area; host pointers.  Returns NULL on failure.
+ * Replaces despeckcl::nlsar_training (include/despeckcl.h:75-83). */
+dcl_stats_collection* dcl_nlsar_training_insar(const float* ampl_master, const float* ampl_slave,
+                                               const float* phase, int height, int width, const int* patch_sizes,
+                                               int n_patch_sizes, const int* scale_sizes, int n_scale_sizes);
+
+/* Training on a covariance image [2*dim*dim][height][width]; dim 2 only.
+ * Replaces despeckcl::nlsar_training (include/despeckcl.h:85-92). */
+dcl_stats_collection* dcl_nlsar_training_covmat(const float* covmat, int height, int width, int dim,
+                                                const int* patch_sizes, int n_patch_sizes, const int* scale_sizes,
+                                                int n_scale_sizes);
+
+/* A one-entry collection with the LUTs of `n` dissimilarities, as the
+ * reference's nlsar::stats::stats(std::vector<float> dissims, unsigned lut_size)
+ * constructor builds them (src/compute/nlsar/stats.cpp:28-80). */
+dcl_stats_collection* dcl_stats_from_dissims(int patch_size, int scale_size, const float* dissims, long n,
+                                             unsigned int lut_size);
+
+int dcl_stats_collection_size(const dcl_stats_collection* c);
+/* Entry i in (patch, scale) order; the pointers stay valid until the collection is freed. */
+int dcl_stats_collection_get(const dcl_stats_collection* c, int i, dcl_stats_entry* out);
+/* A collection holding copies of the given entries. */
+dcl_stats_collection* dcl_stats_collection_from_entries(const dcl_stats_entry* entries, int n);
+void dcl_stats_collection_free(dcl_stats_collection* c);
+
+/* Store / load a statistics collection (despeckcl::store/load_nlsar_stats_collection,
+ * include/despeckcl.h:94-95).  The file is this library's versioned text format;
+ * dcl_stats_load also reads Boost text archives of std::map<nlsar::params,
+ * nlsar::stats> as written by the reference. */
+int dcl_stats_save(const dcl_stats_collection* c, const char* filename);
+dcl_stats_collection* dcl_stats_load(const char* filename);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

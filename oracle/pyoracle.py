@@ -251,3 +251,13 @@ def tile_list(H, W, th, tw, ov):
     w0 = np.zeros(cap, np.int32)
     n = lib().oracle_tile_list(H, W, th, tw, ov, _ip(h0), _ip(w0), cap)
     return list(zip(h0[:n].tolist(), w0[:n].tolist()))
+
+
+def boxcar(a1, a2, phi, window_width, tile=512):
+    a1, a2, phi = _f32(a1), _f32(a2), _f32(phi)
+    H, W = a1.shape
+    ref, ph, coh = (np.zeros((H, W), np.float32) for _ in range(3))
+    rc = lib().oracle_boxcar(_fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), _fp(coh), H, W, window_width, tile)
+    if rc != 0:
+        raise RuntimeError(f"oracle_boxcar failed: {rc}")
+    return ref, ph, coh

@@ -1,0 +1,140 @@
+"""Host-side logic of the C ABI, without a GPU: the library loads, exports every
+entry point its header declares, validates arguments before touching the
+device, builds LUTs and reads/writes statistics files like the reference."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import despeckcl_b200 as dcl
+from despeckcl_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "despeckcl_b200.h")).read()
+    return sorted(set(re.findall(r"\b(dcl_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = dcl.lib()
+    names = declared_symbols()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", api._LIBPATH], capture_output=True, text=True).stdout
+    for n in names:
+        assert re.search(rf"\bT {n}\b", out), n
+
+
+def _stats_entry(p, s):
+    q = np.linspace(0, 1, 256).astype(np.float32)
+    c = np.linspace(0, 100, 256).astype(np.float32)
+    return dcl.Stats(256, 1.0, 10.0, q, c)
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(sws=20), -1),                        # even search window
+    (dict(patches=[4]), -1),                   # even patch size
+    (dict(scales=[2]), -1),                    # even scale size
+    (dict(scales=[11]), -1),                   # scale beyond 9
+    (dict(stats_keys=[(3, 1)]), -2),           # (3, 3) missing
+    (dict(h=0.0), -1),
+])
+def test_argument_validation_happens_on_the_host(kw, code):
+    sws = kw.get("sws", 21)
+    patches = kw.get("patches", [3])
+    scales = kw.get("scales", [1, 3])
+    keys = kw.get("stats_keys", [(p, s) for p in patches for s in scales])
+    stats = {k: _stats_entry(*k) for k in keys}
+    a = np.ones((8, 8), np.float32)
+    with pytest.raises(dcl.DespeckclError) as e:
+        dcl.nlsar_insar(a, a, a, sws, patches, scales, stats, h=kw.get("h", 15.0))
+    assert e.value.code == code
+
+
+def test_covariance_dim3_is_reported_unsupported():
+    cov = np.zeros((3, 3, 4, 4), np.complex64)
+    with pytest.raises(dcl.DespeckclError) as e:
+        dcl.nlsar(cov, 21, [3], [1], {(3, 1): _stats_entry(3, 1)})
+    assert e.value.code == -5
+
+
+def test_lut_builder_matches_oracle(oracle):
+    rng = np.random.default_rng(11)
+    for n, L in [(5000, 256), (10001, 1000), (1234, 256)]:
+        d = rng.gamma(2.0, 2.0, n).astype(np.float32)
+        mine = dcl.stats_from_dissims(d, L)
+        ref = oracle.stats_from_dissims(d, L)
+        assert mine.dissims_min == ref.dissims_min and mine.dissims_max == ref.dissims_max
+        np.testing.assert_array_equal(mine.quantilles, ref.quantilles)
+        np.testing.assert_array_equal(mine.chi2cdf_inv, ref.chi2cdf_inv)
+
+
+def test_chi2_table_matches_scipy():
+    sps = pytest.importorskip("scipy.stats")
+    st = dcl.stats_from_dissims(np.arange(100, dtype=np.float32), 256)
+    ys = np.arange(255) / 256.0
+    np.testing.assert_array_equal(st.chi2cdf_inv[:255], sps.chi2.ppf(ys, 49).astype(np.float32))
+    assert st.chi2cdf_inv[255] == 100000
+
+
+def test_stats_file_round_trip(tmp_path, train_stats):
+    coll = {k: dcl.Stats(v.lut_size, v.dissims_min, v.dissims_max, v.quantilles, v.chi2cdf_inv)
+            for k, v in train_stats.items()}
+    f = str(tmp_path / "nlsar_stats.txt")
+    dcl.store_nlsar_stats_collection(coll, f)
+    back = dcl.load_nlsar_stats_collection(f)
+    assert list(back.keys()) == sorted(coll.keys())
+    for k in coll:
+        a, b = coll[k], back[k]
+        assert (a.lut_size, a.dissims_min, a.dissims_max) == (b.lut_size, b.dissims_min, b.dissims_max)
+        np.testing.assert_array_equal(a.quantilles, b.quantilles)
+        np.testing.assert_array_equal(a.chi2cdf_inv, b.chi2cdf_inv)
+
+
+def test_boost_text_archive_reader(tmp_path):
+    # the shape of a Boost text archive of std::map<nlsar::params, nlsar::stats>:
+    # header, map count, item version, class-info words, then the fields of
+    # parameters.h:51-55 and stats.h:43-50 (vector = count, item version, values)
+    L = 4
+    words = ["22", "serialization::archive", "17", "2", "0", "0", "0", "0",
+             "3", "1", "0", "0", str(L), "1.5", "9.25", str(L), "0", "0", "0.25", "0.5", "1",
+             str(L), "0", "0", "30.5", "45", "100000",
+             "5", "3", str(L), "2", "12", str(L), "0", "0", "0.5", "0.75", "1", str(L), "0", "0", "30.5", "45",
+             "100000"]
+    f = tmp_path / "boost.txt"
+    f.write_text(" ".join(words) + "\n")
+    back = dcl.load_nlsar_stats_collection(str(f))
+    assert list(back.keys()) == [(3, 1), (5, 3)]
+    assert back[(3, 1)].dissims_min == 1.5 and back[(3, 1)].dissims_max == 9.25
+    np.testing.assert_array_equal(back[(5, 3)].quantilles, [0, 0.5, 0.75, 1])
+    np.testing.assert_array_equal(back[(3, 1)].chi2cdf_inv, [0, 30.5, 45, 100000])
+
+
+def test_cpp_api_compiles_and_links(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text(r'''
+#include "despeckcl.h"
+#include <cstdio>
+int main() {
+  nlsar_stats_collection m;
+  std::vector<float> d;
+  for (int i = 0; i < 100; ++i) d.push_back((float)i);
+  m[nlsar::params{3, 1}] = nlsar::stats(d, 256);
+  despeckcl::store_nlsar_stats_collection(m, "s.txt");
+  nlsar_stats_collection b = despeckcl::load_nlsar_stats_collection("s.txt");
+  std::printf("%zu %u %g\n", b.size(), b[nlsar::params{3, 1}].lut_size, b[nlsar::params{3, 1}].dissims_max);
+  return 0;
+}
+''')
+    exe = tmp_path / "use"
+    libdir = os.path.dirname(api._LIBPATH)
+    subprocess.run(["/usr/bin/g++", "-std=c++17", str(src), "-I", os.path.join(ROOT, "include"), "-L", libdir,
+                    "-ldespeckcl_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True, text=True, check=True).stdout
+    assert out.split() == ["1", "256", "99"]

@@ -1,0 +1,224 @@
+"""Parity of the CUDA NL-SAR path with the oracle, through the C ABI.
+
+Tolerances (FP32 against the FP64 oracle): reflectivity and coherence within
+1e-4 relative, phase within 1e-3 rad.  They are asserted on every pixel whose
+FP64 result is well conditioned: no weight of the selected combination within
+1e-3 LUT-index units of a boundary where the weight changes, no weighted
+intensity variance within 1e-4 of zero relative to the squared mean (where the
+reference's alpha formula divides by a vanishing variance), and, in ENL-argmax
+mode, a bias-reduced ENL margin above 1e-4 between the best and second-best
+combination.  On the remaining pixels one LUT bin or one selection may flip
+between any two FP32 implementations (the reference's own OpenCL build
+included); at least 99% of all pixels must still meet the tolerance.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import despeckcl_b200 as dcl  # noqa: E402
+from despeckcl_b200 import synthetic  # noqa: E402
+
+SWS, PATCHES, SCALES = 21, [3, 5, 7], [1, 3]
+REL_TOL, PHASE_TOL = 1e-4, 1e-3
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.init()
+
+
+def run_gpu(a1, a2, ph, stats, mode, sws=SWS, patches=PATCHES, scales=SCALES, selection=False):
+    t = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (a1, a2, ph)]
+    sel = torch.zeros(a1.shape, dtype=torch.int32, device="cuda") if selection else None
+    out = dcl.nlsar_insar_device(*t, sws, patches, scales, stats, select_mode=mode, selection=sel)
+    torch.cuda.synchronize()
+    res = [o.cpu().numpy() for o in out]
+    if selection:
+        res.append(sel.cpu().numpy())
+    return res
+
+
+def wrapped(d):
+    return np.abs(np.angle(np.exp(1j * d.astype(np.float64))))
+
+
+def check_parity(gpu, ora, diag, mode, min_all=0.99):
+    ref_g, ph_g, coh_g = gpu[:3]
+    ref_o, ph_o, coh_o = ora
+    stable = (diag.bin_margin > 1e-3) & (diag.var_cond > 1e-4)
+    if mode == "argmax_enl":
+        stable &= diag.enl_margin > 1e-4
+    e_ref = np.abs(ref_g - ref_o) / np.abs(ref_o)
+    e_coh = np.abs(coh_g - coh_o) / np.maximum(np.abs(coh_o), 1e-3)
+    e_ph = wrapped(ph_g - ph_o)
+    ok = (e_ref <= REL_TOL) & (e_coh <= REL_TOL) & (e_ph <= PHASE_TOL)
+    bad = stable & ~ok
+    assert not bad.any(), (
+        f"{bad.sum()} well-conditioned pixels outside tolerance; worst rel ref {e_ref[stable].max():.3g}, "
+        f"coh {e_coh[stable].max():.3g}, phase {e_ph[stable].max():.3g}; first at {np.argwhere(bad)[:5].tolist()}")
+    assert ok.mean() >= min_all, f"only {ok.mean():.4f} of all pixels within tolerance"
+    assert stable.mean() > 0.5
+    return ok.mean(), stable.mean()
+
+
+@pytest.mark.parametrize("mode", ["reference", "argmax_enl"])
+@pytest.mark.parametrize("shape,seed", [((48, 64), 1), ((33, 70), 2), ((96, 96), 3)])
+def test_nlsar_matches_fp64_oracle(oracle, train_stats, shape, seed, mode):
+    a1, a2, ph = synthetic.insar_scene(*shape, seed)
+    m = 0 if mode == "reference" else 1
+    o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=m, use_double=True, diag=True)
+    g = run_gpu(a1, a2, ph, train_stats, mode, selection=True)
+    check_parity(g, o[:3], o[3], mode)
+    # the per-pixel selection agrees wherever the ENL margin is clear
+    d = o[3]
+    clear = (d.enl_margin > 1e-4) & (d.var_cond > 1e-4) if mode == "argmax_enl" else np.ones(shape, bool)
+    assert np.array_equal(g[3][clear], d.sel[clear])
+
+
+@pytest.mark.parametrize("mode", ["reference", "argmax_enl"])
+def test_nlsar_matches_fp32_oracle(oracle, train_stats, mode):
+    a1, a2, ph = synthetic.insar_scene(64, 80, 4)
+    m = 0 if mode == "reference" else 1
+    o32 = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=m)
+    o64 = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=m, use_double=True,
+                             diag=True)
+    g = run_gpu(a1, a2, ph, train_stats, mode)
+    check_parity(g, o32, o64[3], mode)
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 7), (5, 3), (17, 2)])
+def test_nlsar_degenerate_shapes(oracle, train_stats, shape):
+    a1, a2, ph = synthetic.insar_scene(max(shape[0], 2), max(shape[1], 2), 9)
+    a1, a2, ph = (x[:shape[0], :shape[1]].copy() for x in (a1, a2, ph))
+    o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, use_double=True, diag=True)
+    g = run_gpu(a1, a2, ph, train_stats, "reference")
+    check_parity(g, o[:3], o[3], "reference", min_all=0.0)
+
+
+def test_nlsar_example_parameters(oracle):
+    # the reference example's settings (examples/insar_test.py:43-56):
+    # patches {3,5,7,9,11}, scales {1,3,5}, training on a 25x25 area
+    P, S = [3, 5, 7, 9, 11], [1, 3, 5]
+    t1, t2, tp = synthetic.training_area(25, seed=3)
+    stats = oracle.training_insar(t1, t2, tp, P, S)
+    a1, a2, ph = synthetic.insar_scene(40, 52, 5)
+    for mode, m in (("reference", 0), ("argmax_enl", 1)):
+        o = oracle.nlsar_insar(a1, a2, ph, 21, P, S, stats, select_mode=m, use_double=True, diag=True)
+        g = run_gpu(a1, a2, ph, stats, mode, patches=P, scales=S)
+        check_parity(g, o[:3], o[3], mode)
+
+
+def test_reference_mode_with_extra_stats_key(oracle, train_stats):
+    # a statistics key outside patch_sizes x scale_sizes sorts last: the
+    # reference then filters every pixel with the first combination's weights
+    # and alpha 0 (nlsar_filter_sub_image.cpp:418-422, 537-545)
+    stats = dict(train_stats)
+    stats[(9, 3)] = train_stats[(7, 3)]
+    a1, a2, ph = synthetic.insar_scene(40, 40, 6)
+    o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, stats, use_double=True, diag=True)
+    g = run_gpu(a1, a2, ph, stats, "reference", selection=True)
+    check_parity(g, o[:3], o[3], "reference")
+    assert (g[3] == 0).all()
+
+
+def test_covariance_path_matches_oracle(oracle, train_stats):
+    a1, a2, ph = synthetic.insar_scene(40, 56, 8)
+    cov8 = oracle.covmat_create(a1, a2, ph)
+    # a generic (non-InSAR) covariance: perturb the imaginary diagonal and the
+    # lower off-diagonal so that all 8 planes carry independent data
+    rng = np.random.default_rng(0)
+    cov8[1] = rng.normal(0, 0.1, cov8[1].shape)
+    cov8[4] *= 1.01
+    for mode, m in (("reference", 0), ("argmax_enl", 1)):
+        o = oracle.nlsar_covmat(cov8, SWS, PATCHES, SCALES, train_stats, select_mode=m, use_double=True)
+        cplx = (cov8[0::2] + 1j * cov8[1::2]).reshape(2, 2, 40, 56)
+        g = dcl.nlsar(cplx, SWS, PATCHES, SCALES, train_stats, select_mode=mode)
+        gi = np.empty_like(o)
+        gi[0::2] = g.real.reshape(4, 40, 56)
+        gi[1::2] = g.imag.reshape(4, 40, 56)
+        scale = np.maximum(np.abs(o), np.abs(o[[0, 0, 0, 0, 6, 6, 6, 6]]) * 1e-2)
+        err = np.abs(gi - o) / scale
+        assert (err <= 1e-3).mean() >= 0.99, err.max()
+
+
+def test_host_entry_point_equals_device_entry_point(train_stats):
+    a1, a2, ph = synthetic.insar_scene(70, 90, 10)
+    host = dcl.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode="argmax_enl")
+    dev = run_gpu(a1, a2, ph, train_stats, "argmax_enl")
+    for h, d in zip(host, dev):
+        np.testing.assert_array_equal(h, d)
+
+
+def test_shift_invariance_is_bit_exact(train_stats):
+    # each output pixel depends only on its overlap-radius neighbourhood, so a
+    # crop filtered alone reproduces the interior of the full scene exactly
+    a1, a2, ph = synthetic.insar_scene(200, 260, 12)
+    full = run_gpu(a1, a2, ph, train_stats, "argmax_enl")
+    y0, x0, h, w = 37, 61, 90, 120
+    crop = run_gpu(*(x[y0:y0 + h, x0:x0 + w].copy() for x in (a1, a2, ph)), train_stats, "argmax_enl")
+    ov = 14
+    for f, c in zip(full, crop):
+        np.testing.assert_array_equal(c[ov:h - ov - 1, ov:w - ov - 1],
+                                      f[y0 + ov:y0 + h - ov - 1, x0 + ov:x0 + w - ov - 1])
+
+
+def test_batched_launch_equals_single_scenes(train_stats):
+    shapes = [(64, 96), (130, 70), (33, 200)]
+    scenes = [synthetic.insar_scene(h, w, 20 + i) for i, (h, w) in enumerate(shapes)]
+    tens = [tuple(torch.from_numpy(x).cuda() for x in s) for s in scenes]
+    outs = dcl.nlsar_insar_batch_device(tens, SWS, PATCHES, SCALES, train_stats, select_mode="argmax_enl")
+    torch.cuda.synchronize()
+    for s, o in zip(scenes, outs):
+        single = run_gpu(*s, train_stats, "argmax_enl")
+        for a, b in zip(o, single):
+            np.testing.assert_array_equal(a.cpu().numpy(), b)
+
+
+def test_constant_scene_is_a_fixed_point(train_stats):
+    a = np.full((64, 64), 2.0, np.float32)
+    z = np.full((64, 64), 0.5, np.float32)
+    ref, ph, coh = run_gpu(a, a, z, train_stats, "argmax_enl")
+    np.testing.assert_allclose(ref, 4.0, rtol=1e-5)
+    np.testing.assert_allclose(ph, 0.5, atol=1e-5)
+    np.testing.assert_allclose(coh, 1.0, rtol=1e-5)
+
+
+def test_config1_scene_reference_mode(oracle, train_stats):
+    # the 512 x 512 scene of the first benchmark configuration, seed 1
+    a1, a2, ph = synthetic.insar_scene(512, 512, 1)
+    o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=0, use_double=True,
+                           diag=True)
+    g = run_gpu(a1, a2, ph, train_stats, "reference")
+    frac_ok, frac_stable = check_parity(g, o[:3], o[3], "reference")
+    print(f"config-1 reference mode: {frac_ok:.5f} within tolerance, {frac_stable:.3f} well conditioned")
+
+
+def test_boxcar_matches_oracle(oracle):
+    a1, a2, ph = synthetic.insar_scene(300, 530, 13)
+    for w in (1, 3, 5, 7):
+        o = oracle.boxcar(a1, a2, ph, w)
+        g = dcl.boxcar(a1, a2, ph, w)
+        np.testing.assert_allclose(g[0], o[0], rtol=1e-5)
+        np.testing.assert_array_less(wrapped(g[1] - o[1]), 1e-4)
+        np.testing.assert_allclose(g[2], o[2], rtol=1e-4, atol=1e-6)
+
+
+def test_training_matches_oracle(oracle):
+    t1, t2, tp = synthetic.training_area(128, seed=7)
+    mine = dcl.nlsar_train_insar(t1, t2, tp, PATCHES, SCALES)
+    ref = oracle.training_insar(t1, t2, tp, PATCHES, SCALES)
+    assert sorted(mine.keys()) == sorted(ref.keys())
+    for k in ref:
+        a, b = mine[k], ref[k]
+        n = 128 - k[1] + 1
+        npatch = (-(-n // k[0])) ** 2
+        npairs = npatch * (npatch - 1) // 2
+        assert a.lut_size == 256
+        assert a.dissims_min == pytest.approx(b.dissims_min, rel=1e-5)
+        assert a.dissims_max == pytest.approx(b.dissims_max, rel=1e-5)
+        assert np.abs(a.quantilles - b.quantilles).max() <= 5.0 / npairs + 1e-7
+        np.testing.assert_array_equal(a.chi2cdf_inv, b.chi2cdf_inv)
