@@ -124,4 +124,9 @@ __global__ void prep_scale_kernel(const float4* cori, int Hp, int Wp, int pitch,
 cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, int grid,
                                cudaStream_t st);
 
+// The compile-time specialised kernel (nlsar_fast.cu) for the common
+// configurations; fast_kernel_supported() tells whether `F` has one.
+bool fast_kernel_supported(const FilterParams& F);
+cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st);
+
 }  // namespace dcl

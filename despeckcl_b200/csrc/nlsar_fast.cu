@@ -1,0 +1,381 @@
+// Fused NL-SAR tile kernel specialised at compile time on the search-window
+// half size and the patch half sizes of a pass (the common configurations),
+// for sm_100a.  Same semantics as the generic kernel in nlsar_kernels.cu.
+//
+// Per CTA: a 32 x 32 output tile, 8 warps, each thread owning 4 vertically
+// consecutive pixels of one column.  For every scale the search-window offsets
+// are taken three at a time along a row of the window (same dy, consecutive
+// dx, so a thread's neighbour loads overlap across the batch):
+//   A  GLR similarities of the batch on the tile plus the patch halo
+//      (each thread: two adjacent pixels x three offsets from four neighbour
+//      loads); reference order of the two pixels in the measure is kept
+//      (center first in the upper half, neighbour first in the mirrored half,
+//      compute_pixel_similarities_2x2.cl.in:54-71, copy_symm_weights.cl:56-76)
+//   B  horizontal sums for all patch sizes of the pass at once (nested
+//      rings), packed as float4 per pixel
+//   C  vertical sums, composite LUT weight (compute_weights.cl:40-51), and
+//      register accumulation of sum w, sum w^2, sum w I_d, sum w I_d^2,
+//      sum w Re C01, sum w Im C01 per patch size; the centre offset has weight
+//      1 (routines.cpp:151-157)
+// then ENL, alpha, bias-reduced ENL and the selection (compute_nl_statistics.cl,
+// compute_alphas.cl, compute_enls_nobias.cl, best_params.cpp) and the blended
+// weighted mean (weighted_means.cl:79), decomposed (covmat_decompose.cl:32-37).
+// Every sum is evaluated in a fixed order relative to its output pixel, so a
+// pixel's result does not depend on where tiles fall (shift invariant).
+
+#include <cuda_runtime.h>
+
+#include "nlsar_common.cuh"
+
+namespace dcl {
+
+namespace {
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+template <int WSH, int PH0, int PH1, int PH2>
+struct Fast {
+  static constexpr int NP = (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
+  static constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
+  static constexpr int SWS = 2 * WSH + 1;
+  static constexpr int TH = 32, TW = 32, PX = 4;
+  static constexpr int K = 3;                       // offsets per batch (SWS % K == 0)
+  static constexpr int RS = TW + 2 * (PHM + WSH);   // scaled covariance region (square)
+  static constexpr int RO = TW + 2 * WSH;           // original covariance region
+  static constexpr int SIMW = TW + 2 * PHM;         // similarity region (square)
+  static constexpr int SIMP = SIMW + 1;             // odd pitch: conflict-free row runs
+  static constexpr int RUNS = (SIMW + 1) / 2;       // two-pixel runs per similarity row
+  static constexpr int LUTREP = 4;                  // interleaved LUT copies (bank spread)
+  static constexpr int HROWS = PX + 2 * PHM;        // horizontal-sum rows a thread reads
+  // shared memory, in 4-byte words
+  static constexpr int OFF_CS = 0;
+  static constexpr int OFF_CO = OFF_CS + 4 * RS * RS;
+  static constexpr int OFF_H = OFF_CO + 4 * RO * RO;
+  static constexpr int OFF_LD = OFF_H + 4 * K * SIMW * TW;
+  static constexpr int OFF_SIM = OFF_LD + RS * RS;
+  static constexpr int OFF_LUT = OFF_SIM + K * SIMW * SIMP;
+  static constexpr int WORDS = OFF_LUT + NP * kMaxLut * LUTREP;
+  static_assert(SWS % K == 0, "offset batches must tile a window row");
+  static_assert(PH0 >= 0, "at least one patch");
+};
+
+__device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 b, float lb, bool lower, float c2d) {
+  // sim_measures.h:52-64 with nlooks 1; ld of each pixel precomputed
+  const float s00 = a.x + b.x, s11 = a.y + b.y, sre = a.z + b.z, sim = a.w + b.w;
+  const float det = (s00 * s11) - (sre * sre + sim * sim);
+  const float t = lower ? (c2d + lb) + la : (c2d + la) + lb;
+  float r = -(t - 2.0f * __logf(det));
+  if (r != r) r = 0.0f;
+  return r;
+}
+
+template <int WSH, int PH0, int PH1, int PH2>
+__global__ void __launch_bounds__(kThreads, 1)
+    nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
+  using C = Fast<WSH, PH0, PH1, PH2>;
+  constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RO = C::RO;
+  constexpr int SIMW = C::SIMW, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
+  constexpr int PH[3] = {PH0, PH1, PH2};
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  float4* sCs = reinterpret_cast<float4*>(smem + C::OFF_CS);
+  float4* sCo = reinterpret_cast<float4*>(smem + C::OFF_CO);
+  float4* sH = reinterpret_cast<float4*>(smem + C::OFF_H);
+  float* sLd = smem + C::OFF_LD;
+  float* sSim = smem + C::OFF_SIM;
+  float* sLut = smem + C::OFF_LUT;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int y0 = warp * PX;
+  const float c2d = P.c2d;
+
+  for (int tile = blockIdx.x; tile < P.total_tiles; tile += gridDim.x) {
+    int lo = 0, hi = P.n_scenes - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (scenes[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    const SceneDesc& S = scenes[lo];
+    const int lt = tile - S.tile_begin;
+    const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
+    const int vy0 = ty * C::TH, vx0 = tx * TW;
+    const int G = P.G, pitch = S.pitch;
+
+    __syncthreads();
+    for (int i = tid; i < RO * RO; i += kThreads) {
+      const int r = i / RO, c = i - r * RO;
+      sCo[i] = S.cori[(size_t)(vy0 - WSH + r + G) * pitch + (vx0 - WSH + c + G)];
+    }
+
+    float acc[PX][NP][8];
+    float best_e[PX], best_a[PX], best_s0[PX], best_m[PX][4];
+    int best_rank[PX], best_combo[PX];
+#pragma unroll
+    for (int i = 0; i < PX; ++i) {
+      best_e[i] = -1.0f;
+      best_rank[i] = 0x7fffffff;
+      best_combo[i] = -1;
+      best_a[i] = 0.f;
+      best_s0[i] = 1.f;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) best_m[i][d] = 0.f;
+    }
+
+    int loaded_slot = -1;
+    for (int ps = 0; ps < P.npass; ++ps) {
+      const PassParams& pp = P.pass[ps];
+      __syncthreads();
+      if (pp.scale_slot != loaded_slot) {
+        const float4* cs = S.cs[pp.scale_slot];
+        const float* ldp = S.ld[pp.scale_slot];
+        const int by = vy0 - PHM - WSH + G, bx = vx0 - PHM - WSH + G;
+        for (int i = tid; i < RS * RS; i += kThreads) {
+          const int r = i / RS, c = i - r * RS;
+          const size_t g = (size_t)(by + r) * pitch + (bx + c);
+          sCs[i] = cs[g];
+          sLd[i] = ldp[g];
+        }
+        loaded_slot = pp.scale_slot;
+      }
+      // composite weight tables, LUTREP interleaved copies
+      for (int i = tid; i < NP * kMaxLut * C::LUTREP; i += kThreads) {
+        const int j = i / (kMaxLut * C::LUTREP);
+        const int e = (i - j * kMaxLut * C::LUTREP) / C::LUTREP;
+        sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
+      }
+      float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        const ComboParams& cp = P.combo[pp.combo[j]];
+        inv_span[j] = 1.0f / cp.span;
+        nbias[j] = -cp.dmin * inv_span[j];
+        lm1[j] = cp.lm1;
+        dmax[j] = cp.dmax;
+      }
+#pragma unroll
+      for (int i = 0; i < PX; ++i)
+#pragma unroll
+        for (int j = 0; j < NP; ++j)
+#pragma unroll
+          for (int a = 0; a < 8; ++a) acc[i][j][a] = 0.f;
+      __syncthreads();
+
+      for (int dy = -WSH; dy <= WSH; ++dy) {
+        for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
+          // ---- A: similarities of offsets (dy, dx0..dx0+K-1)
+          for (int it = tid; it < SIMW * C::RUNS; it += kThreads) {
+            const int r = it / C::RUNS;
+            const int c0 = 2 * (it - r * C::RUNS);
+            const int ci = (r + WSH) * RS + (c0 + WSH);
+            const float4 a0 = sCs[ci], a1 = sCs[ci + 1];
+            const float la0 = sLd[ci], la1 = sLd[ci + 1];
+            const int ni = ci + dy * RS + dx0;
+            float4 nb[K + 1];
+            float nl[K + 1];
+#pragma unroll
+            for (int j = 0; j <= K; ++j) {
+              nb[j] = sCs[ni + j];
+              nl[j] = sLd[ni + j];
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+              const int dx = dx0 + k;
+              const bool lower = (dy > 0) || (dy == 0 && dx > 0);
+              float* dst = sSim + (k * SIMW + r) * SIMP + c0;
+              dst[0] = glr_sim(a0, la0, nb[k], nl[k], lower, c2d);
+              if (c0 + 1 < SIMW) dst[1] = glr_sim(a1, la1, nb[k + 1], nl[k + 1], lower, c2d);
+            }
+          }
+          __syncthreads();
+          // ---- B: horizontal sums, 4 output columns per item
+          for (int it = tid; it < K * SIMW * (TW / 4); it += kThreads) {
+            const int k = it / (SIMW * (TW / 4));
+            const int rem = it - k * (SIMW * (TW / 4));
+            const int r = rem >> 3, seg = rem & 7;
+            const float* row = sSim + (k * SIMW + r) * SIMP + 4 * seg;
+            float s[4 + 2 * PHM];
+#pragma unroll
+            for (int j = 0; j < 4 + 2 * PHM; ++j) s[j] = row[j];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              float h[3] = {0.f, 0.f, 0.f};
+              float ring = s[o + PHM];
+#pragma unroll
+              for (int j = 0; j < 3; ++j)
+                if (PH[j] == 0) h[j] = ring;
+#pragma unroll
+              for (int b = 1; b <= PHM; ++b) {
+                ring += s[o + PHM - b] + s[o + PHM + b];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                  if (PH[j] == b) h[j] = ring;
+              }
+              sH[(k * SIMW + r) * TW + 4 * seg + o] = make_float4(h[0], h[1], h[2], 0.f);
+            }
+          }
+          __syncthreads();
+          // ---- C: vertical sums, weights, accumulation
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int dx = dx0 + k;
+            const float4* col = sH + (k * SIMW + y0) * TW + lane;
+            float4 hv[C::HROWS];
+#pragma unroll
+            for (int j = 0; j < C::HROWS; ++j) hv[j] = col[j * TW];
+            float w[PX][NP];
+            if (dy == 0 && dx == 0) {
+#pragma unroll
+              for (int i = 0; i < PX; ++i)
+#pragma unroll
+                for (int j = 0; j < NP; ++j) w[i][j] = 1.0f;
+            } else {
+#pragma unroll
+              for (int i = 0; i < PX; ++i) {
+#pragma unroll
+                for (int j = 0; j < NP; ++j) {
+                  float d = 0.f;
+#pragma unroll
+                  for (int a = -PH[j]; a <= PH[j]; ++a) {
+                    const float4 v = hv[i + PHM + a];
+                    d += (j == 0) ? v.x : ((j == 1) ? v.y : v.z);
+                  }
+                  // (unsigned)((clamp(d)-dmin)/(dmax-dmin)*(L-1)) by a saturating
+                  // FMA and a round-toward-zero add; d > dmax has weight 0
+                  const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
+                  const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
+                  const int idx = __float_as_int(t) - 0x4B000000;
+                  const float lw = sLut[(j * kMaxLut + idx) * C::LUTREP + (lane & (C::LUTREP - 1))];
+                  w[i][j] = (d > dmax[j]) ? 0.0f : lw;
+                }
+              }
+            }
+#pragma unroll
+            for (int i = 0; i < PX; ++i) {
+              const float4 v = sCo[(y0 + i + WSH + dy) * RO + (lane + WSH + dx)];
+              const float x2 = v.x * v.x, y2 = v.y * v.y;
+#pragma unroll
+              for (int j = 0; j < NP; ++j) {
+                float* A = acc[i][j];
+                const float ww = w[i][j];
+                A[0] += ww;
+                A[1] = fmaf(ww, ww, A[1]);
+                A[2] = fmaf(ww, v.x, A[2]);
+                A[3] = fmaf(ww, v.y, A[3]);
+                A[4] = fmaf(ww, x2, A[4]);
+                A[5] = fmaf(ww, y2, A[5]);
+                A[6] = fmaf(ww, v.z, A[6]);
+                A[7] = fmaf(ww, v.w, A[7]);
+              }
+            }
+          }
+          __syncthreads();
+        }
+      }
+
+      // ---- statistics, alpha, ENL', selection
+#pragma unroll
+      for (int i = 0; i < PX; ++i) {
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          const float* A = acc[i][j];
+          const float s0 = A[0], s1 = A[1], s2 = A[2], s3 = A[3], s4 = A[4], s5 = A[5], s6 = A[6], s7 = A[7];
+          const float enl = s0 * s0 / s1;
+          const float i0 = s2 / s0, i1 = s3 / s0;
+          const float v0 = s4 / s0 - i0 * i0, v1 = s5 / s0 - i1 * i1;
+          float alpha = 0.0f;
+          alpha = fmaxf(alpha, fmaxf(0.0f, (v0 - i0 * i0) / v0));
+          alpha = fmaxf(alpha, fmaxf(0.0f, (v1 - i1 * i1) / v1));
+          if (P.alpha_zero) alpha = 0.0f;
+          const float oma = 1.0f - alpha;
+          const float enb = enl / (oma * oma + (alpha * alpha + 2.0f * alpha * (1.0f - alpha) / s0) * enl);
+          const int combo = pp.combo[j];
+          const int rank = P.combo[combo].rank;
+          const bool take = (P.select_mode == 0) || (enb > best_e[i]) || (enb == best_e[i] && rank < best_rank[i]);
+          const bool take_fb = !take && best_combo[i] < 0 && combo == P.fallback_combo;
+          if (take) {
+            best_e[i] = enb;
+            best_rank[i] = rank;
+          }
+          if (take || take_fb) {
+            best_combo[i] = combo;
+            best_a[i] = alpha;
+            best_s0[i] = s0;
+            best_m[i][0] = s2;
+            best_m[i][1] = s3;
+            best_m[i][2] = s6;
+            best_m[i][3] = s7;
+          }
+        }
+      }
+    }
+
+    // ---- blend with the centre, decompose, store
+#pragma unroll
+    for (int i = 0; i < PX; ++i) {
+      const int y = y0 + i;
+      const int vy = vy0 + y, vx = vx0 + lane;
+      const int oy = (vy < S.H - 1) ? vy : (vy == S.vH ? S.H - 1 : -1);
+      const int ox = (vx < S.W - 1) ? vx : (vx == S.vW ? S.W - 1 : -1);
+      if (oy < 0 || ox < 0) continue;
+      const float4 c = sCo[(y + WSH) * RO + (lane + WSH)];
+      const float alpha = best_a[i], s0 = best_s0[i];
+      const float oma = 1.0f - alpha;
+      const float c00 = oma * best_m[i][0] / s0 + alpha * c.x;
+      const float c11 = oma * best_m[i][1] / s0 + alpha * c.y;
+      const float cre = oma * best_m[i][2] / s0 + alpha * c.z;
+      const float cim = oma * best_m[i][3] / s0 + alpha * c.w;
+      const size_t o = (size_t)oy * S.W + ox;
+      const float am = sqrtf(c00), as = sqrtf(c11);
+      const float r = 0.5f * (am + as);
+      S.ref[o] = r * r;
+      S.phase[o] = atan2f(cim, cre);
+      S.coh[o] = sqrtf(cim * cim + cre * cre) / (am * as);
+      if (S.sel_out) S.sel_out[o] = best_combo[i];
+    }
+  }
+}
+
+template <int WSH, int PH0, int PH1, int PH2>
+cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
+  using C = Fast<WSH, PH0, PH1, PH2>;
+  const size_t smem = (size_t)C::WORDS * 4;
+  static bool configured = false;
+  if (!configured) {
+    const cudaError_t e = cudaFuncSetAttribute(nlsar_fast_kernel<WSH, PH0, PH1, PH2>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  nlsar_fast_kernel<WSH, PH0, PH1, PH2><<<grid, kThreads, smem, st>>>(F, d_scenes);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Specialisations available: the search window 21 (half 10) with every pass
+// holding the patch halves {1,2,3} (patches 3,5,7) or the single half 1, 2 or
+// 3 (reference mode).  Returns false when no specialisation matches.
+bool fast_kernel_supported(const FilterParams& F) {
+  if (F.wsh != 10 || F.npass < 1) return false;
+  const PassParams& p0 = F.pass[0];
+  for (int i = 0; i < F.npass; ++i) {
+    const PassParams& p = F.pass[i];
+    if (p.np != p0.np) return false;
+    for (int j = 0; j < p.np; ++j)
+      if (p.ph[j] != p0.ph[j]) return false;
+  }
+  if (p0.np == 3) return p0.ph[0] == 1 && p0.ph[1] == 2 && p0.ph[2] == 3;
+  if (p0.np == 1) return p0.ph[0] >= 1 && p0.ph[0] <= 3;
+  return false;
+}
+
+cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
+  const PassParams& p0 = F.pass[0];
+  if (p0.np == 3) return launch_fast_t<10, 1, 2, 3>(F, d_scenes, grid, st);
+  switch (p0.ph[0]) {
+    case 1: return launch_fast_t<10, 1, -1, -1>(F, d_scenes, grid, st);
+    case 2: return launch_fast_t<10, 2, -1, -1>(F, d_scenes, grid, st);
+    default: return launch_fast_t<10, 3, -1, -1>(F, d_scenes, grid, st);
+  }
+}
+
+}  // namespace dcl

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -340,6 +341,12 @@ struct ProfileState {
   long launches = 0;  // all kernels launched by the library while profiling
 };
 static thread_local ProfileState g_prof;
+// DESPECKCL_B200_GENERIC=1 routes every call to the generic kernel (used by
+// the tests to check both kernels against each other)
+static const bool g_force_generic = [] {
+  const char* s = std::getenv("DESPECKCL_B200_GENERIC");
+  return s && s[0] == '1';
+}();
 
 void profile_count(int n) {
   if (g_prof.on) g_prof.launches += n;
@@ -377,7 +384,9 @@ int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scene
     cudaEventCreate(&b);
     cudaEventRecord(a, st);
   }
-  const cudaError_t e = launch_nlsar_fused(pl.full8, F, d_scenes, smem, F.total_tiles, st);
+  const bool fast = !pl.full8 && !g_force_generic && fast_kernel_supported(F);
+  const cudaError_t e = fast ? launch_nlsar_fast(F, d_scenes, F.total_tiles, st)
+                             : launch_nlsar_fused(pl.full8, F, d_scenes, smem, F.total_tiles, st);
   if (g_prof.on) {
     cudaEventRecord(b, st);
     g_prof.ev.push_back({a, b});

@@ -180,6 +180,7 @@ template <typename T> struct ComboResult {
   std::vector<T> mean8;       // 8 planes of sum(w*C)/sum(w) over the core
   std::vector<T> bin_margin;  // FP64 diagnostics: min distance of a LUT index to a bin edge
   std::vector<T> var_cond;    // FP64 diagnostics: min over d of |var_d| / I_d^2 (alpha conditioning)
+  std::vector<T> kappa;       // FP64 diagnostics: sum w|C01| / |sum w C01| (cancellation in the complex mean)
 };
 
 struct LutView {
@@ -240,7 +241,7 @@ template <typename T> struct TileOut {
   int hc = 0, wc = 0;
   std::vector<T> cov8;       // [8][hc][wc]
   std::vector<int> sel;      // selected combo index (loop order: scale outer, patch inner)
-  std::vector<T> bin_margin, enl_margin, var_cond;
+  std::vector<T> bin_margin, enl_margin, var_cond, kappa;
 };
 
 // nlsar_filter_sub_image.cpp:146-390 for one padded tile `ori`.
@@ -357,6 +358,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
       if (P.want_diag) {
         R.bin_margin.assign(nc, std::numeric_limits<T>::infinity());
         R.var_cond.assign(nc, std::numeric_limits<T>::infinity());
+        R.kappa.assign(nc, T(1));
       }
       for (int y = 0; y < hc; ++y)
         for (int x = 0; x < wc; ++x) {
@@ -409,6 +411,17 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
             R.mean8[(size_t)pl * nc + o] = cnew;
             (void)ws;
           }
+          if (P.want_diag) {
+            T mag = 0;
+            for (int a = 0; a < sws; ++a)
+              for (int b = 0; b < sws; ++b) {
+                const T w = wfull[(size_t)(a * sws + b) * nc + o];
+                const int ny = y + a + Ssh + Psh, nx = x + b + Ssh + Psh;
+                mag += std::fabs(w) * std::hypot(ori.at(2, ny, nx), ori.at(3, ny, nx));
+              }
+            const T sr = R.mean8[(size_t)2 * nc + o], si = R.mean8[(size_t)3 * nc + o];
+            R.kappa[o] = mag / std::hypot(sr, si);
+          }
         }
     }
   }
@@ -428,6 +441,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
     out.bin_margin.assign(nc, 0);
     out.enl_margin.assign(nc, std::numeric_limits<T>::infinity());
     out.var_cond.assign(nc, std::numeric_limits<T>::infinity());
+    out.kappa.assign(nc, T(1));
   }
   // combos ranked in map order for the argmax
   std::vector<int> map_order;
@@ -479,6 +493,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
     }
     if (P.want_diag) {
       out.bin_margin[o] = res[sel].bin_margin[o];
+      out.kappa[o] = res[sel].kappa[o];
       // reference mode depends on the selected combination only; the ENL
       // argmax depends on every combination's alpha
       if (P.select_mode == 0)
@@ -545,7 +560,7 @@ int get_overlap(const FilterParams& P) {
 template <typename T>
 int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w, int nthreads,
                 Cov<T>& outc, std::vector<int>* sel, std::vector<T>* bmar, std::vector<T>* emar,
-                std::vector<T>* vcond) {
+                std::vector<T>* vcond, std::vector<T>* kap = nullptr) {
   const int ov = get_overlap(P);
   const int H = img.h, W = img.w;
   if (tile_h <= 2 * ov || tile_w <= 2 * ov) return -1;
@@ -564,6 +579,7 @@ int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w
   if (bmar) bmar->assign((size_t)H * W, 0);
   if (emar) emar->assign((size_t)H * W, 0);
   if (vcond) vcond->assign((size_t)H * W, 0);
+  if (kap) kap->assign((size_t)H * W, 0);
   for (size_t t = 0; t < tiles.size(); ++t) {
     const TileOut<T>& o = outs[t];
     // the core of a tile of size tile_h x tile_w starts at tile origin + ov;
@@ -579,6 +595,7 @@ int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w
         if (bmar && !o.bin_margin.empty()) (*bmar)[(size_t)yy * W + xx] = o.bin_margin[oi];
         if (emar && !o.enl_margin.empty()) (*emar)[(size_t)yy * W + xx] = o.enl_margin[oi];
         if (vcond && !o.var_cond.empty()) (*vcond)[(size_t)yy * W + xx] = o.var_cond[oi];
+        if (kap && !o.kappa.empty()) (*kap)[(size_t)yy * W + xx] = o.kappa[oi];
       }
   }
   return 0;
@@ -615,13 +632,13 @@ int build_params(FilterParams& P, int sws, const int* patches, int np, const int
 template <typename T>
 int run_insar(const float* a1, const float* a2, const float* ph, float* ref, float* phase, float* coh,
               int H, int W, const FilterParams& P, int tile_h, int tile_w, int nthreads, int* sel,
-              double* bmar, double* emar, double* vcond) {
+              double* bmar, double* emar, double* vcond, double* kappa) {
   const Cov<T> img = covmat_create<T>(a1, a2, ph, H, W);
   Cov<T> outc;
   std::vector<int> s;
-  std::vector<T> b, e, v;
+  std::vector<T> b, e, v, k;
   int rc = nlsar_image<T>(img, P, tile_h, tile_w, nthreads, outc, sel ? &s : nullptr, bmar ? &b : nullptr,
-                          emar ? &e : nullptr, vcond ? &v : nullptr);
+                          emar ? &e : nullptr, vcond ? &v : nullptr, kappa ? &k : nullptr);
   if (rc) return rc;
   for (int y = 0; y < H; ++y)
     for (int x = 0; x < W; ++x) {
@@ -632,6 +649,7 @@ int run_insar(const float* a1, const float* a2, const float* ph, float* ref, flo
       if (bmar) bmar[i] = (double)b[i];
       if (emar) emar[i] = (double)e[i];
       if (vcond) vcond[i] = (double)v[i];
+      if (kappa) kappa[i] = (double)k[i];
     }
   return 0;
 }
@@ -659,17 +677,17 @@ extern "C" int oracle_nlsar_insar(const float* a1, const float* a2, const float*
                                   const int* scales, int ns, const oracle_lut* luts, int nluts, float h,
                                   float c, int select_mode, int use_double, int tile_h, int tile_w,
                                   int nthreads, int* sel, double* bin_margin, double* enl_margin,
-                                  double* var_cond) {
+                                  double* var_cond, double* kappa) {
   FilterParams P;
-  const int want_diag = (bin_margin || enl_margin || var_cond) ? 1 : 0;
+  const int want_diag = (bin_margin || enl_margin || var_cond || kappa) ? 1 : 0;
   int rc = build_params(P, sws, patches, np, scales, ns, luts, nluts, h, c, select_mode, want_diag);
   if (rc) return rc;
   if (H < 1 || W < 1) return -1;
   if (use_double)
     return run_insar<double>(a1, a2, ph, ref, phase, coh, H, W, P, tile_h, tile_w, nthreads, sel, bin_margin,
-                             enl_margin, var_cond);
+                             enl_margin, var_cond, kappa);
   return run_insar<float>(a1, a2, ph, ref, phase, coh, H, W, P, tile_h, tile_w, nthreads, sel, bin_margin,
-                          enl_margin, var_cond);
+                          enl_margin, var_cond, kappa);
 }
 
 extern "C" int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int sws, const int* patches,

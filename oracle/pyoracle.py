@@ -125,15 +125,16 @@ def nlsar_insar(a1, a2, phi, sws, patches, scales, stats, h=15.0, c=49.0, select
     bm = np.zeros((H, W), np.float64) if diag else None
     em = np.zeros((H, W), np.float64) if diag else None
     vc = np.zeros((H, W), np.float64) if diag else None
+    kp = np.zeros((H, W), np.float64) if diag else None
     rc = lib().oracle_nlsar_insar(
         _fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), _fp(coh), H, W, sws, _ip(p), len(p), _ip(s), len(s),
         luts, len(stats), ctypes.c_float(h), ctypes.c_float(c), select_mode, int(use_double), th, tw, nthreads,
         _ip(sel) if diag else None, _dp(bm) if diag else None, _dp(em) if diag else None,
-        _dp(vc) if diag else None)
+        _dp(vc) if diag else None, _dp(kp) if diag else None)
     if rc != 0:
         raise RuntimeError(f"oracle_nlsar_insar failed: {rc}")
     if diag:
-        return ref, ph, coh, Diagnostics(sel, bm, em, vc)
+        return ref, ph, coh, Diagnostics(sel, bm, em, vc, kp)
     return ref, ph, coh
 
 
@@ -163,13 +164,17 @@ class Diagnostics:
     enl_margin relative gap between the best and second-best ENL' (argmax mode)
     var_cond   min over the two intensities of |weighted variance| / mean^2;
                near 0 the reference's alpha formula is ill-conditioned
+    kappa      sum w |C01| / |sum w C01| over the selected weights: the
+               cancellation factor of the weighted complex mean, which scales
+               the FP32 rounding error of coherence and phase
     """
 
-    def __init__(self, sel, bin_margin, enl_margin, var_cond):
+    def __init__(self, sel, bin_margin, enl_margin, var_cond, kappa):
         self.sel = sel
         self.bin_margin = bin_margin
         self.enl_margin = enl_margin
         self.var_cond = var_cond
+        self.kappa = kappa
 
 
 class OracleStats:
