@@ -7,8 +7,8 @@
 // are taken three at a time along a row of the window (same dy, consecutive
 // dx, so a thread's neighbour loads overlap across the batch):
 //   A  GLR similarities of the batch on the tile plus the patch halo
-//      (each thread: two adjacent pixels x three offsets from four neighbour
-//      loads); reference order of the two pixels in the measure is kept
+//      (each thread: one pixel x three offsets); reference order of the two
+//      pixels in the measure is kept
 //      (center first in the upper half, neighbour first in the mirrored half,
 //      compute_pixel_similarities_2x2.cl.in:54-71, copy_symm_weights.cl:56-76)
 //   B  horizontal sums for all patch sizes of the pass at once (nested
@@ -44,14 +44,14 @@ struct Fast {
   static constexpr int RO = TW + 2 * WSH;           // original covariance region
   static constexpr int SIMW = TW + 2 * PHM;         // similarity region (square)
   static constexpr int SIMP = SIMW + 1;             // odd pitch: conflict-free row runs
-  static constexpr int RUNS = (SIMW + 1) / 2;       // two-pixel runs per similarity row
-  static constexpr int LUTREP = 4;                  // interleaved LUT copies (bank spread)
+  static constexpr int HP = TW + 1;                 // horizontal-sum row pitch (float4): conflict-free stores
+  static constexpr int LUTREP = 8;                  // interleaved LUT copies (bank spread)
   static constexpr int HROWS = PX + 2 * PHM;        // horizontal-sum rows a thread reads
   // shared memory, in 4-byte words
   static constexpr int OFF_CS = 0;
   static constexpr int OFF_CO = OFF_CS + 4 * RS * RS;
   static constexpr int OFF_H = OFF_CO + 4 * RO * RO;
-  static constexpr int OFF_LD = OFF_H + 4 * K * SIMW * TW;
+  static constexpr int OFF_LD = OFF_H + 4 * K * SIMW * HP;
   static constexpr int OFF_SIM = OFF_LD + RS * RS;
   static constexpr int OFF_LUT = OFF_SIM + K * SIMW * SIMP;
   static constexpr int WORDS = OFF_LUT + NP * kMaxLut * LUTREP;
@@ -161,55 +161,58 @@ __global__ void __launch_bounds__(kThreads, 1)
 
       for (int dy = -WSH; dy <= WSH; ++dy) {
         for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
-          // ---- A: similarities of offsets (dy, dx0..dx0+K-1)
-          for (int it = tid; it < SIMW * C::RUNS; it += kThreads) {
-            const int r = it / C::RUNS;
-            const int c0 = 2 * (it - r * C::RUNS);
-            const int ci = (r + WSH) * RS + (c0 + WSH);
-            const float4 a0 = sCs[ci], a1 = sCs[ci + 1];
-            const float la0 = sLd[ci], la1 = sLd[ci + 1];
+          // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
+          // thread and consecutive pixels on consecutive lanes (conflict free)
+          // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
+          constexpr int SIMW8 = (SIMW + 7) / 8 * 8;
+          for (int it = tid; it < SIMW * SIMW8; it += kThreads) {
+            const int r = it / SIMW8;
+            const int c = it - r * SIMW8;
+            if (c >= SIMW) continue;
+            const int ci = (r + WSH) * RS + (c + WSH);
+            const float4 a = sCs[ci];
+            const float la = sLd[ci];
             const int ni = ci + dy * RS + dx0;
-            float4 nb[K + 1];
-            float nl[K + 1];
-#pragma unroll
-            for (int j = 0; j <= K; ++j) {
-              nb[j] = sCs[ni + j];
-              nl[j] = sLd[ni + j];
-            }
 #pragma unroll
             for (int k = 0; k < K; ++k) {
               const int dx = dx0 + k;
               const bool lower = (dy > 0) || (dy == 0 && dx > 0);
-              float* dst = sSim + (k * SIMW + r) * SIMP + c0;
-              dst[0] = glr_sim(a0, la0, nb[k], nl[k], lower, c2d);
-              if (c0 + 1 < SIMW) dst[1] = glr_sim(a1, la1, nb[k + 1], nl[k + 1], lower, c2d);
+              sSim[(k * SIMW + r) * SIMP + c] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], lower, c2d);
             }
           }
           __syncthreads();
-          // ---- B: horizontal sums, 4 output columns per item
-          for (int it = tid; it < K * SIMW * (TW / 4); it += kThreads) {
-            const int k = it / (SIMW * (TW / 4));
-            const int rem = it - k * (SIMW * (TW / 4));
-            const int r = rem >> 3, seg = rem & 7;
-            const float* row = sSim + (k * SIMW + r) * SIMP + 4 * seg;
-            float s[4 + 2 * PHM];
+          // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
+          // quad of rows x 8 column segments; lanes are ordered so that each
+          // quarter warp's float4 stores hit 8 distinct bank groups.
+          {
+            constexpr int QUADS = (SIMW + 3) / 4;
+            const int r_off = lane & 3;
+            const int seg = ((lane >> 3) << 1) | ((lane >> 2) & 1);
+            for (int q = warp; q < K * QUADS; q += kWarps) {
+              const int k = q / QUADS;
+              const int r = (q - k * QUADS) * 4 + r_off;
+              if (r < SIMW) {
+                const float* row = sSim + (k * SIMW + r) * SIMP + 4 * seg;
+                float s[4 + 2 * PHM];
 #pragma unroll
-            for (int j = 0; j < 4 + 2 * PHM; ++j) s[j] = row[j];
+                for (int j = 0; j < 4 + 2 * PHM; ++j) s[j] = row[j];
 #pragma unroll
-            for (int o = 0; o < 4; ++o) {
-              float h[3] = {0.f, 0.f, 0.f};
-              float ring = s[o + PHM];
+                for (int o = 0; o < 4; ++o) {
+                  float h[3] = {0.f, 0.f, 0.f};
+                  float ring = s[o + PHM];
 #pragma unroll
-              for (int j = 0; j < 3; ++j)
-                if (PH[j] == 0) h[j] = ring;
+                  for (int j = 0; j < 3; ++j)
+                    if (PH[j] == 0) h[j] = ring;
 #pragma unroll
-              for (int b = 1; b <= PHM; ++b) {
-                ring += s[o + PHM - b] + s[o + PHM + b];
+                  for (int b = 1; b <= PHM; ++b) {
+                    ring += s[o + PHM - b] + s[o + PHM + b];
 #pragma unroll
-                for (int j = 0; j < 3; ++j)
-                  if (PH[j] == b) h[j] = ring;
+                    for (int j = 0; j < 3; ++j)
+                      if (PH[j] == b) h[j] = ring;
+                  }
+                  sH[(k * SIMW + r) * C::HP + 4 * seg + o] = make_float4(h[0], h[1], h[2], 0.f);
+                }
               }
-              sH[(k * SIMW + r) * TW + 4 * seg + o] = make_float4(h[0], h[1], h[2], 0.f);
             }
           }
           __syncthreads();
@@ -217,10 +220,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int k = 0; k < K; ++k) {
             const int dx = dx0 + k;
-            const float4* col = sH + (k * SIMW + y0) * TW + lane;
+            const float4* col = sH + (k * SIMW + y0) * C::HP + lane;
             float4 hv[C::HROWS];
 #pragma unroll
-            for (int j = 0; j < C::HROWS; ++j) hv[j] = col[j * TW];
+            for (int j = 0; j < C::HROWS; ++j) hv[j] = col[j * C::HP];
             float w[PX][NP];
             if (dy == 0 && dx == 0) {
 #pragma unroll
@@ -243,8 +246,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                   const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
                   const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
                   const int idx = __float_as_int(t) - 0x4B000000;
-                  const float lw = sLut[(j * kMaxLut + idx) * C::LUTREP + (lane & (C::LUTREP - 1))];
-                  w[i][j] = (d > dmax[j]) ? 0.0f : lw;
+                  // lanes past the cut-off skip the table (fewer bank conflicts)
+                  float lw = 0.0f;
+                  if (d <= dmax[j] || d != d)
+                    lw = sLut[(j * kMaxLut + idx) * C::LUTREP + (lane & (C::LUTREP - 1))];
+                  w[i][j] = lw;
                 }
               }
             }

@@ -241,7 +241,7 @@ template <typename T> struct TileOut {
   int hc = 0, wc = 0;
   std::vector<T> cov8;       // [8][hc][wc]
   std::vector<int> sel;      // selected combo index (loop order: scale outer, patch inner)
-  std::vector<T> bin_margin, enl_margin, var_cond, kappa;
+  std::vector<T> bin_margin, enl_margin, var_cond, kappa, bin_margin_all;
 };
 
 // nlsar_filter_sub_image.cpp:146-390 for one padded tile `ori`.
@@ -442,6 +442,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
     out.enl_margin.assign(nc, std::numeric_limits<T>::infinity());
     out.var_cond.assign(nc, std::numeric_limits<T>::infinity());
     out.kappa.assign(nc, T(1));
+    out.bin_margin_all.assign(nc, std::numeric_limits<T>::infinity());
   }
   // combos ranked in map order for the argmax
   std::vector<int> map_order;
@@ -494,6 +495,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
     if (P.want_diag) {
       out.bin_margin[o] = res[sel].bin_margin[o];
       out.kappa[o] = res[sel].kappa[o];
+      for (int ci = 0; ci < nco; ++ci) out.bin_margin_all[o] = std::min(out.bin_margin_all[o], res[ci].bin_margin[o]);
       // reference mode depends on the selected combination only; the ENL
       // argmax depends on every combination's alpha
       if (P.select_mode == 0)
@@ -560,7 +562,7 @@ int get_overlap(const FilterParams& P) {
 template <typename T>
 int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w, int nthreads,
                 Cov<T>& outc, std::vector<int>* sel, std::vector<T>* bmar, std::vector<T>* emar,
-                std::vector<T>* vcond, std::vector<T>* kap = nullptr) {
+                std::vector<T>* vcond, std::vector<T>* kap = nullptr, std::vector<T>* bma = nullptr) {
   const int ov = get_overlap(P);
   const int H = img.h, W = img.w;
   if (tile_h <= 2 * ov || tile_w <= 2 * ov) return -1;
@@ -580,6 +582,7 @@ int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w
   if (emar) emar->assign((size_t)H * W, 0);
   if (vcond) vcond->assign((size_t)H * W, 0);
   if (kap) kap->assign((size_t)H * W, 0);
+  if (bma) bma->assign((size_t)H * W, 0);
   for (size_t t = 0; t < tiles.size(); ++t) {
     const TileOut<T>& o = outs[t];
     // the core of a tile of size tile_h x tile_w starts at tile origin + ov;
@@ -596,6 +599,7 @@ int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w
         if (emar && !o.enl_margin.empty()) (*emar)[(size_t)yy * W + xx] = o.enl_margin[oi];
         if (vcond && !o.var_cond.empty()) (*vcond)[(size_t)yy * W + xx] = o.var_cond[oi];
         if (kap && !o.kappa.empty()) (*kap)[(size_t)yy * W + xx] = o.kappa[oi];
+        if (bma && !o.bin_margin_all.empty()) (*bma)[(size_t)yy * W + xx] = o.bin_margin_all[oi];
       }
   }
   return 0;
@@ -632,13 +636,13 @@ int build_params(FilterParams& P, int sws, const int* patches, int np, const int
 template <typename T>
 int run_insar(const float* a1, const float* a2, const float* ph, float* ref, float* phase, float* coh,
               int H, int W, const FilterParams& P, int tile_h, int tile_w, int nthreads, int* sel,
-              double* bmar, double* emar, double* vcond, double* kappa) {
+              double* bmar, double* emar, double* vcond, double* kappa, double* bma) {
   const Cov<T> img = covmat_create<T>(a1, a2, ph, H, W);
   Cov<T> outc;
   std::vector<int> s;
-  std::vector<T> b, e, v, k;
+  std::vector<T> b, e, v, k, ba;
   int rc = nlsar_image<T>(img, P, tile_h, tile_w, nthreads, outc, sel ? &s : nullptr, bmar ? &b : nullptr,
-                          emar ? &e : nullptr, vcond ? &v : nullptr, kappa ? &k : nullptr);
+                          emar ? &e : nullptr, vcond ? &v : nullptr, kappa ? &k : nullptr, bma ? &ba : nullptr);
   if (rc) return rc;
   for (int y = 0; y < H; ++y)
     for (int x = 0; x < W; ++x) {
@@ -650,6 +654,7 @@ int run_insar(const float* a1, const float* a2, const float* ph, float* ref, flo
       if (emar) emar[i] = (double)e[i];
       if (vcond) vcond[i] = (double)v[i];
       if (kappa) kappa[i] = (double)k[i];
+      if (bma) bma[i] = (double)ba[i];
     }
   return 0;
 }
@@ -677,17 +682,17 @@ extern "C" int oracle_nlsar_insar(const float* a1, const float* a2, const float*
                                   const int* scales, int ns, const oracle_lut* luts, int nluts, float h,
                                   float c, int select_mode, int use_double, int tile_h, int tile_w,
                                   int nthreads, int* sel, double* bin_margin, double* enl_margin,
-                                  double* var_cond, double* kappa) {
+                                  double* var_cond, double* kappa, double* bin_margin_all) {
   FilterParams P;
-  const int want_diag = (bin_margin || enl_margin || var_cond || kappa) ? 1 : 0;
+  const int want_diag = (bin_margin || enl_margin || var_cond || kappa || bin_margin_all) ? 1 : 0;
   int rc = build_params(P, sws, patches, np, scales, ns, luts, nluts, h, c, select_mode, want_diag);
   if (rc) return rc;
   if (H < 1 || W < 1) return -1;
   if (use_double)
     return run_insar<double>(a1, a2, ph, ref, phase, coh, H, W, P, tile_h, tile_w, nthreads, sel, bin_margin,
-                             enl_margin, var_cond, kappa);
+                             enl_margin, var_cond, kappa, bin_margin_all);
   return run_insar<float>(a1, a2, ph, ref, phase, coh, H, W, P, tile_h, tile_w, nthreads, sel, bin_margin,
-                          enl_margin, var_cond, kappa);
+                          enl_margin, var_cond, kappa, bin_margin_all);
 }
 
 extern "C" int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int sws, const int* patches,

@@ -22,7 +22,7 @@ int oracle_nlsar_insar(const float* a1, const float* a2, const float* ph, float*
                        int H, int W, int sws, const int* patches, int np, const int* scales, int ns,
                        const oracle_lut* luts, int nluts, float h, float c, int select_mode, int use_double,
                        int tile_h, int tile_w, int nthreads, int* sel, double* bin_margin, double* enl_margin,
-                       double* var_cond, double* kappa);
+                       double* var_cond, double* kappa, double* bin_margin_all);
 int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int sws, const int* patches, int np,
                         const int* scales, int ns, const oracle_lut* luts, int nluts, float h, float c,
                         int select_mode, int use_double, int tile_h, int tile_w, int nthreads);

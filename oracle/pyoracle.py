@@ -126,15 +126,16 @@ def nlsar_insar(a1, a2, phi, sws, patches, scales, stats, h=15.0, c=49.0, select
     em = np.zeros((H, W), np.float64) if diag else None
     vc = np.zeros((H, W), np.float64) if diag else None
     kp = np.zeros((H, W), np.float64) if diag else None
+    ba = np.zeros((H, W), np.float64) if diag else None
     rc = lib().oracle_nlsar_insar(
         _fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), _fp(coh), H, W, sws, _ip(p), len(p), _ip(s), len(s),
         luts, len(stats), ctypes.c_float(h), ctypes.c_float(c), select_mode, int(use_double), th, tw, nthreads,
         _ip(sel) if diag else None, _dp(bm) if diag else None, _dp(em) if diag else None,
-        _dp(vc) if diag else None, _dp(kp) if diag else None)
+        _dp(vc) if diag else None, _dp(kp) if diag else None, _dp(ba) if diag else None)
     if rc != 0:
         raise RuntimeError(f"oracle_nlsar_insar failed: {rc}")
     if diag:
-        return ref, ph, coh, Diagnostics(sel, bm, em, vc, kp)
+        return ref, ph, coh, Diagnostics(sel, bm, em, vc, kp, ba)
     return ref, ph, coh
 
 
@@ -167,9 +168,13 @@ class Diagnostics:
     kappa      sum w |C01| / |sum w C01| over the selected weights: the
                cancellation factor of the weighted complex mean, which scales
                the FP32 rounding error of coherence and phase
+    bin_margin_all  bin_margin minimised over every combination (a flip in a
+               non-selected combination moves its ENL' and can change the
+               argmax selection)
     """
 
-    def __init__(self, sel, bin_margin, enl_margin, var_cond, kappa):
+    def __init__(self, sel, bin_margin, enl_margin, var_cond, kappa, bin_margin_all):
+        self.bin_margin_all = bin_margin_all
         self.sel = sel
         self.bin_margin = bin_margin
         self.enl_margin = enl_margin

@@ -83,10 +83,13 @@ def test_nlsar_matches_fp64_oracle(oracle, train_stats, shape, seed, mode):
     o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=m, use_double=True, diag=True)
     g = run_gpu(a1, a2, ph, train_stats, mode, selection=True)
     check_parity(g, o[:3], o[3], mode)
-    # the per-pixel selection agrees wherever the ENL margin is clear
+    # the per-pixel selection agrees wherever the ENL margin is clear and no
+    # weight of any combination sits within 1e-3 index units of a LUT edge
     d = o[3]
-    clear = (d.enl_margin > 1e-4) & (d.var_cond > 1e-4) if mode == "argmax_enl" else np.ones(shape, bool)
+    clear = ((d.enl_margin > 1e-4) & (d.var_cond > 1e-4) & (d.bin_margin_all > 1e-3)
+             if mode == "argmax_enl" else np.ones(shape, bool))
     assert np.array_equal(g[3][clear], d.sel[clear])
+    assert (g[3] == d.sel).mean() >= 0.995
 
 
 @pytest.mark.parametrize("mode", ["reference", "argmax_enl"])
