@@ -24,6 +24,7 @@
 #include "../../include/despeckcl_b200.h"
 #include "dcl_internal.h"
 #include "nlsar_common.cuh"
+#include "nlsar_plan.h"
 
 namespace dcl {
 
@@ -74,17 +75,6 @@ float rescale_gamma_2x2() {
   // covmat_rescale.cl:25-26 with nlooks = 1, dimension = 2
   return std::pow(std::min(1.0f / 2.0f, 1.0f), 0.33333f);
 }
-
-struct Plan {
-  FilterParams P;
-  std::vector<float> wtab;
-  std::vector<int> scales;       // distinct scale sizes, caller order (scale slots)
-  std::vector<char> slot_used;   // slots referenced by the passes
-  int overlap = 0;
-  int shm = 0;                   // largest scale half among used slots
-  bool full8 = false;
-  int px = 4;
-};
 
 static int validate_sizes(int sws, const int* patches, int np, const int* scales, int ns, std::vector<int>& P,
                           std::vector<int>& S) {
@@ -273,11 +263,6 @@ int choose_k(const Plan& pl, size_t& smem_bytes) {
   }
   return 0;
 }
-
-// Geometry of one scene on the virtual plane.
-struct SceneGeom {
-  int H, W, vH, vW, tiles_x, tiles_y, Hp, Wp, pitch;
-};
 
 SceneGeom scene_geom(const Plan& pl, int H, int W) {
   SceneGeom g;

@@ -1,0 +1,41 @@
+// Host-side plan of an NL-SAR call and the helpers that stage and launch it
+// (defined in nlsar_host.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/despeckcl_b200.h"
+#include "nlsar_common.cuh"
+
+namespace dcl {
+
+// Validated parameters of one call, ready for the kernels.
+struct Plan {
+  FilterParams P;
+  std::vector<float> wtab;
+  std::vector<int> scales;       // distinct scale sizes, caller order (scale slots)
+  std::vector<char> slot_used;   // slots referenced by the passes
+  int overlap = 0;
+  int shm = 0;                   // largest scale half among used slots
+  bool full8 = false;
+  int px = 4;
+};
+
+// Geometry of one scene on the virtual plane.
+struct SceneGeom {
+  int H, W, vH, vW, tiles_x, tiles_y, Hp, Wp, pitch;
+};
+
+int make_plan(int sws, const int* patches, int np, const int* scales, int ns, const dcl_stats_entry* stats,
+              int nstats, float h, float c, int select_mode, bool full8, Plan& pl);
+int choose_k(const Plan& pl, size_t& smem_bytes);
+SceneGeom scene_geom(const Plan& pl, int H, int W);
+size_t scratch_bytes(const Plan& pl, const SceneGeom& g);
+void carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d);
+int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
+                const float* phi, const float* cov_in, cudaStream_t st);
+int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st);
+
+}  // namespace dcl

@@ -95,6 +95,23 @@ int dcl_nlsar_insar_device(const float* ampl_master, const float* ampl_slave, co
                            const dcl_stats_entry* stats, int n_stats, float h_param, float c_param,
                            int select_mode, int* selection_out, void* stream);
 
+/* NL-SAR on device pointers without allocating device memory.  No
+ * counterpart in the reference: it exists for callers that cannot allocate
+ * GPU memory while they filter (a fixed memory budget, a host framework that
+ * owns the allocator, or code that must not grow the pool mid-stream).  Same
+ * arguments and results as dcl_nlsar_insar_device; the scratch is a 64 MiB
+ * static device array shared by all calls on a device, so scenes whose padded
+ * frame does not fit are rejected with DCL_ERR_INVALID_ARGUMENT (about
+ * 1000 x 1000 pixels with search 21, patches {3,5,7}, scales {1,3}), and calls
+ * that overlap on the GPU race.  The first call on a device resolves the
+ * array's address: make it before any stream capture. */
+int dcl_nlsar_insar_device_noalloc(const float* ampl_master, const float* ampl_slave, const float* phase,
+                                   float* ref_filt, float* phase_filt, float* coh_filt, int height, int width,
+                                   int search_window_size, const int* patch_sizes, int n_patch_sizes,
+                                   const int* scale_sizes, int n_scale_sizes, const dcl_stats_entry* stats,
+                                   int n_stats, float h_param, float c_param, int select_mode, int* selection_out,
+                                   void* stream);
+
 /* NL-SAR on a covariance image [2*dim*dim][height][width] (even planes real,
  * odd planes imaginary), host pointers.  dim 2 only (dim 3 returns
  * DCL_ERR_UNSUPPORTED).  Replaces despeckcl::nlsar (include/despeckcl.h:62-73). */
