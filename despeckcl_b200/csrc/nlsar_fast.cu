@@ -2,7 +2,7 @@
 // half size and the patch half sizes of a pass (the common configurations),
 // for sm_100a.  Same semantics as the generic kernel in nlsar_kernels.cu.
 //
-// Per CTA: a 32 x 32 output tile, 8 warps, each thread owning 4 vertically
+// Per CTA: a 32 x 32 output tile, 16 warps, each thread owning 2 vertically
 // consecutive pixels of one column.  For every scale the search-window offsets
 // are taken three at a time along a row of the window (same dy, consecutive
 // dx, so a thread's neighbour loads overlap across the batch):
@@ -12,7 +12,7 @@
 //      (center first in the upper half, neighbour first in the mirrored half,
 //      compute_pixel_similarities_2x2.cl.in:54-71, copy_symm_weights.cl:56-76)
 //   B  horizontal sums for all patch sizes of the pass at once (nested
-//      rings), packed as float4 per pixel
+//      rings), one plane per patch size
 //   C  vertical sums, composite LUT weight (compute_weights.cl:40-51), and
 //      register accumulation of sum w, sum w^2, sum w I_d, sum w I_d^2,
 //      sum w Re C01, sum w Im C01 per patch size; the centre offset has weight
@@ -38,20 +38,21 @@ struct Fast {
   static constexpr int NP = (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
   static constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
   static constexpr int SWS = 2 * WSH + 1;
-  static constexpr int TH = 32, TW = 32, PX = 4;
+  static constexpr int TH = 32, TW = 32, PX = 2;   // 2 vertically adjacent pixels per thread
+  static constexpr int WARPS = TH / PX, THREADS = 32 * WARPS;
   static constexpr int K = 3;                       // offsets per batch (SWS % K == 0)
   static constexpr int RS = TW + 2 * (PHM + WSH);   // scaled covariance region (square)
   static constexpr int RO = TW + 2 * WSH;           // original covariance region
   static constexpr int SIMW = TW + 2 * PHM;         // similarity region (square)
   static constexpr int SIMP = SIMW + 1;             // odd pitch: conflict-free row runs
-  static constexpr int HP = TW + 1;                 // horizontal-sum row pitch (float4): conflict-free stores
+  static constexpr int HP = TW + 1;                 // horizontal-sum row pitch (words): conflict-free stores
+  static constexpr int HPL = K * SIMW * HP;         // one patch size's horizontal-sum plane
   static constexpr int LUTREP = 8;                  // interleaved LUT copies (bank spread)
-  static constexpr int HROWS = PX + 2 * PHM;        // horizontal-sum rows a thread reads
   // shared memory, in 4-byte words
   static constexpr int OFF_CS = 0;
   static constexpr int OFF_CO = OFF_CS + 4 * RS * RS;
   static constexpr int OFF_H = OFF_CO + 4 * RO * RO;
-  static constexpr int OFF_LD = OFF_H + 4 * K * SIMW * HP;
+  static constexpr int OFF_LD = OFF_H + NP * HPL;
   static constexpr int OFF_SIM = OFF_LD + RS * RS;
   static constexpr int OFF_LUT = OFF_SIM + K * SIMW * SIMP;
   static constexpr int WORDS = OFF_LUT + NP * kMaxLut * LUTREP;
@@ -69,18 +70,24 @@ __device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 
   return r;
 }
 
+// patch half size of pass component j (compile time)
+template <int PH0, int PH1, int PH2>
+__device__ __forceinline__ constexpr int ph_of(int j) {
+  return j == 0 ? PH0 : (j == 1 ? PH1 : PH2);
+}
+
 template <int WSH, int PH0, int PH1, int PH2>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
   using C = Fast<WSH, PH0, PH1, PH2>;
   constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RO = C::RO;
   constexpr int SIMW = C::SIMW, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
-  constexpr int PH[3] = {PH0, PH1, PH2};
+  constexpr int NT = C::THREADS, NW = C::WARPS;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
   float4* sCs = reinterpret_cast<float4*>(smem + C::OFF_CS);
   float4* sCo = reinterpret_cast<float4*>(smem + C::OFF_CO);
-  float4* sH = reinterpret_cast<float4*>(smem + C::OFF_H);
+  float* sH = smem + C::OFF_H;  // [NP][K][SIMW][HP]
   float* sLd = smem + C::OFF_LD;
   float* sSim = smem + C::OFF_SIM;
   float* sLut = smem + C::OFF_LUT;
@@ -101,7 +108,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int G = P.G, pitch = S.pitch;
 
     __syncthreads();
-    for (int i = tid; i < RO * RO; i += kThreads) {
+    for (int i = tid; i < RO * RO; i += NT) {
       const int r = i / RO, c = i - r * RO;
       sCo[i] = S.cori[(size_t)(vy0 - WSH + r + G) * pitch + (vx0 - WSH + c + G)];
     }
@@ -128,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const float4* cs = S.cs[pp.scale_slot];
         const float* ldp = S.ld[pp.scale_slot];
         const int by = vy0 - PHM - WSH + G, bx = vx0 - PHM - WSH + G;
-        for (int i = tid; i < RS * RS; i += kThreads) {
+        for (int i = tid; i < RS * RS; i += NT) {
           const int r = i / RS, c = i - r * RS;
           const size_t g = (size_t)(by + r) * pitch + (bx + c);
           sCs[i] = cs[g];
@@ -137,12 +144,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         loaded_slot = pp.scale_slot;
       }
       // composite weight tables, LUTREP interleaved copies
-      for (int i = tid; i < NP * kMaxLut * C::LUTREP; i += kThreads) {
+      for (int i = tid; i < NP * kMaxLut * C::LUTREP; i += NT) {
         const int j = i / (kMaxLut * C::LUTREP);
         const int e = (i - j * kMaxLut * C::LUTREP) / C::LUTREP;
         sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
       }
-      float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
+      float inv_span[NP], nbias[NP], lm1[NP], dmax[NP], dmin[NP], w0[NP];
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         const ComboParams& cp = P.combo[pp.combo[j]];
@@ -150,6 +157,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         nbias[j] = -cp.dmin * inv_span[j];
         lm1[j] = cp.lm1;
         dmax[j] = cp.dmax;
+        dmin[j] = cp.dmin;
+        w0[j] = P.wtab[pp.combo[j] * kMaxLut];  // weight of LUT index 0 (d <= dmin, or NaN)
       }
 #pragma unroll
       for (int i = 0; i < PX; ++i)
@@ -165,7 +174,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           // thread and consecutive pixels on consecutive lanes (conflict free)
           // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
           constexpr int SIMW8 = (SIMW + 7) / 8 * 8;
-          for (int it = tid; it < SIMW * SIMW8; it += kThreads) {
+          for (int it = tid; it < SIMW * SIMW8; it += NT) {
             const int r = it / SIMW8;
             const int c = it - r * SIMW8;
             if (c >= SIMW) continue;
@@ -188,7 +197,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             constexpr int QUADS = (SIMW + 3) / 4;
             const int r_off = lane & 3;
             const int seg = ((lane >> 3) << 1) | ((lane >> 2) & 1);
-            for (int q = warp; q < K * QUADS; q += kWarps) {
+            for (int q = warp; q < K * QUADS; q += NW) {
               const int k = q / QUADS;
               const int r = (q - k * QUADS) * 4 + r_off;
               if (r < SIMW) {
@@ -202,15 +211,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                   float ring = s[o + PHM];
 #pragma unroll
                   for (int j = 0; j < 3; ++j)
-                    if (PH[j] == 0) h[j] = ring;
+                    if (ph_of<PH0, PH1, PH2>(j) == 0) h[j] = ring;
 #pragma unroll
                   for (int b = 1; b <= PHM; ++b) {
                     ring += s[o + PHM - b] + s[o + PHM + b];
 #pragma unroll
                     for (int j = 0; j < 3; ++j)
-                      if (PH[j] == b) h[j] = ring;
+                      if (ph_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
                   }
-                  sH[(k * SIMW + r) * C::HP + 4 * seg + o] = make_float4(h[0], h[1], h[2], 0.f);
+#pragma unroll
+                  for (int j = 0; j < NP; ++j) sH[j * C::HPL + (k * SIMW + r) * C::HP + 4 * seg + o] = h[j];
                 }
               }
             }
@@ -220,11 +230,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int k = 0; k < K; ++k) {
             const int dx = dx0 + k;
-            const float4* col = sH + (k * SIMW + y0) * C::HP + lane;
-            float4 hv[C::HROWS];
-#pragma unroll
-            for (int j = 0; j < C::HROWS; ++j) hv[j] = col[j * C::HP];
             float w[PX][NP];
+            // vertical windows: patch j needs rows y0+PHM-ph_of<PH0, PH1, PH2>(j) .. y0+PHM+PX-1+ph_of<PH0, PH1, PH2>(j)
+            float hv[NP][PX + 2 * PHM];
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+              const float* col = sH + j * C::HPL + (k * SIMW + y0 + PHM - ph_of<PH0, PH1, PH2>(j)) * C::HP + lane;
+#pragma unroll
+              for (int r = 0; r < PX + 2 * ph_of<PH0, PH1, PH2>(j); ++r) hv[j][r] = col[r * C::HP];
+            }
             if (dy == 0 && dx == 0) {
 #pragma unroll
               for (int i = 0; i < PX; ++i)
@@ -237,18 +251,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int j = 0; j < NP; ++j) {
                   float d = 0.f;
 #pragma unroll
-                  for (int a = -PH[j]; a <= PH[j]; ++a) {
-                    const float4 v = hv[i + PHM + a];
-                    d += (j == 0) ? v.x : ((j == 1) ? v.y : v.z);
-                  }
+                  for (int a = -ph_of<PH0, PH1, PH2>(j); a <= ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + ph_of<PH0, PH1, PH2>(j) + a];
                   // (unsigned)((clamp(d)-dmin)/(dmax-dmin)*(L-1)) by a saturating
                   // FMA and a round-toward-zero add; d > dmax has weight 0
                   const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
                   const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
                   const int idx = __float_as_int(t) - 0x4B000000;
-                  // lanes past the cut-off skip the table (fewer bank conflicts)
-                  float lw = 0.0f;
-                  if (d <= dmax[j] || d != d)
+                  // only lanes strictly inside (dmin, dmax] read the table: at or
+                  // below dmin (and for NaN) the index is 0, above dmax the
+                  // weight is 0 (fewer bank conflicts)
+                  float lw = (d > dmax[j]) ? 0.0f : w0[j];
+                  if (d > dmin[j] && d <= dmax[j])
                     lw = sLut[(j * kMaxLut + idx) * C::LUTREP + (lane & (C::LUTREP - 1))];
                   w[i][j] = lw;
                 }
@@ -351,7 +364,7 @@ cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int 
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  nlsar_fast_kernel<WSH, PH0, PH1, PH2><<<grid, kThreads, smem, st>>>(F, d_scenes);
+  nlsar_fast_kernel<WSH, PH0, PH1, PH2><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
   return cudaGetLastError();
 }
 
