@@ -7,8 +7,9 @@
 // are taken three at a time along a row of the window (same dy, consecutive
 // dx, so a thread's neighbour loads overlap across the batch):
 //   A  GLR similarities of the batch on the tile plus the patch halo
-//      (each thread: one pixel x three offsets); reference order of the two
-//      pixels in the measure is kept
+//      (each thread: one pixel x three offsets); the measure is evaluated in
+//      an order symmetric in its two pixels, so the mirrored half window gets
+//      exactly the values of the reference's copy
 //      (center first in the upper half, neighbour first in the mirrored half,
 //      compute_pixel_similarities_2x2.cl.in:54-71, copy_symm_weights.cl:56-76)
 //   B  horizontal sums for all patch sizes of the pass at once (nested
@@ -60,12 +61,14 @@ struct Fast {
   static_assert(PH0 >= 0, "at least one patch");
 };
 
-__device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 b, float lb, bool lower, float c2d) {
-  // sim_measures.h:52-64 with nlooks 1; ld of each pixel precomputed
+__device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 b, float lb, float c2d) {
+  // sim_measures.h:52-64 with nlooks 1 and the per-pixel ln det precomputed:
+  // -(2 d ln 2 + ln det A + ln det B - 2 ln det(A+B)); NaN -> 0.  The two ln det
+  // terms are added first, which makes the value exactly symmetric in (A, B).
   const float s00 = a.x + b.x, s11 = a.y + b.y, sre = a.z + b.z, sim = a.w + b.w;
   const float det = (s00 * s11) - (sre * sre + sim * sim);
-  const float t = lower ? (c2d + lb) + la : (c2d + la) + lb;
-  float r = -(t - 2.0f * __logf(det));
+  const float t = (la + lb) + c2d;
+  float r = fmaf(2.0f * 0.69314718f, __log2f(det), -t);
   if (r != r) r = 0.0f;
   return r;
 }
@@ -149,7 +152,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
         const int e = (i - j * kMaxLut * C::LUTREP) / C::LUTREP;
         sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
       }
-      float inv_span[NP], nbias[NP], lm1[NP], dmax[NP], dmin[NP], w0[NP];
+      float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         const ComboParams& cp = P.combo[pp.combo[j]];
@@ -157,9 +160,11 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
         nbias[j] = -cp.dmin * inv_span[j];
         lm1[j] = cp.lm1;
         dmax[j] = cp.dmax;
-        dmin[j] = cp.dmin;
-        w0[j] = P.wtab[pp.combo[j] * kMaxLut];  // weight of LUT index 0 (d <= dmin, or NaN)
       }
+      // this lane's copy of the table of component j
+      const float* lut_j[NP];
+#pragma unroll
+      for (int j = 0; j < NP; ++j) lut_j[j] = sLut + j * kMaxLut * C::LUTREP + (lane & (C::LUTREP - 1));
 #pragma unroll
       for (int i = 0; i < PX; ++i)
 #pragma unroll
@@ -183,11 +188,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
             const float la = sLd[ci];
             const int ni = ci + dy * RS + dx0;
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const int dx = dx0 + k;
-              const bool lower = (dy > 0) || (dy == 0 && dx > 0);
-              sSim[(k * SIMW + r) * SIMP + c] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], lower, c2d);
-            }
+            for (int k = 0; k < K; ++k) sSim[(k * SIMW + r) * SIMP + c] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
           }
           __syncthreads();
           // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
@@ -254,16 +255,15 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
                   for (int a = -ph_of<PH0, PH1, PH2>(j); a <= ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + ph_of<PH0, PH1, PH2>(j) + a];
                   // (unsigned)((clamp(d)-dmin)/(dmax-dmin)*(L-1)) by a saturating
                   // FMA and a round-toward-zero add; d > dmax has weight 0
+                  // index = (unsigned)((clamp(d) - dmin) / (dmax - dmin) * (L - 1)):
+                  // a saturating FMA clamps (and maps NaN to 0), a round-toward-zero
+                  // add of 2^23 truncates, and the float's low mantissa bits are the
+                  // index; d > dmax has weight 0
                   const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
                   const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
                   const int idx = __float_as_int(t) - 0x4B000000;
-                  // only lanes strictly inside (dmin, dmax] read the table: at or
-                  // below dmin (and for NaN) the index is 0, above dmax the
-                  // weight is 0 (fewer bank conflicts)
-                  float lw = (d > dmax[j]) ? 0.0f : w0[j];
-                  if (d > dmin[j] && d <= dmax[j])
-                    lw = sLut[(j * kMaxLut + idx) * C::LUTREP + (lane & (C::LUTREP - 1))];
-                  w[i][j] = lw;
+                  const float lw = lut_j[j][idx * C::LUTREP];
+                  w[i][j] = (d > dmax[j]) ? 0.0f : lw;
                 }
               }
             }
