@@ -7,6 +7,7 @@ from .api import (  # noqa: F401
     DEFAULT_LOG_LEVELS,
     SELECT_MODES,
     DespeckclError,
+    NlsarBatch,
     Params,
     Stats,
     StatsCollection,

@@ -60,8 +60,12 @@ def lib() -> ctypes.CDLL:
         L.dcl_last_error.restype = ctypes.c_char_p
         L.dcl_version.restype = ctypes.c_char_p
         for fn in ("dcl_nlsar_training_insar", "dcl_nlsar_training_covmat", "dcl_stats_load",
-                   "dcl_stats_collection_from_entries", "dcl_stats_from_dissims"):
+                   "dcl_stats_collection_from_entries", "dcl_stats_from_dissims", "dcl_nlsar_batch_create"):
             getattr(L, fn).restype = ctypes.c_void_p
+        L.dcl_nlsar_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.dcl_nlsar_batch_variant.argtypes = [ctypes.c_void_p]
+        L.dcl_nlsar_batch_launches.argtypes = [ctypes.c_void_p]
+        L.dcl_nlsar_batch_destroy.argtypes = [ctypes.c_void_p]
         L.dcl_stats_collection_size.argtypes = [ctypes.c_void_p]
         L.dcl_stats_collection_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StatsEntry)]
         L.dcl_stats_collection_free.argtypes = [ctypes.c_void_p]
@@ -339,6 +343,60 @@ def nlsar_insar_batch_device(scenes, search_window_size, patch_sizes, scale_size
                                               nsn, arr, ns, ctypes.c_float(h), ctypes.c_float(c), _mode(select_mode),
                                               _stream(stream)))
     return outs
+
+
+class NlsarBatch:
+    """A prepared batch (dcl_nlsar_batch_*): scenes of uneven size filtered by
+    one fused launch per run, optionally replayed as a CUDA graph and with the
+    kernel instantiation picked by the autotuner."""
+
+    def __init__(self, scenes, search_window_size, patch_sizes, scale_sizes, nlsar_stats, h=15.0, c=49.0,
+                 select_mode="argmax_enl", outs=None, graph=True, autotune=True, variant=None, stream=None):
+        import torch
+
+        n = len(scenes)
+        self.scenes = scenes
+        self.outs = outs if outs is not None else [
+            tuple(torch.empty(s[0].shape, dtype=torch.float32, device=s[0].device) for _ in range(3)) for s in scenes]
+        P = ctypes.c_void_p * n
+        ptr = lambda i, j, src: _dptr(src[i][j])
+        args = [P(*[ptr(i, j, scenes) for i in range(n)]) for j in range(3)]
+        args += [P(*[ptr(i, j, self.outs) for i in range(n)]) for j in range(3)]
+        hs = (ctypes.c_int * n)(*[s[0].shape[0] for s in scenes])
+        ws = (ctypes.c_int * n)(*[s[0].shape[1] for s in scenes])
+        pk, pp, npn = _ints(patch_sizes)
+        sk, sp, nsn = _ints(scale_sizes)
+        arr, ns, keep = _entries(nlsar_stats)
+        flags = (1 if graph else 0) | (2 if autotune else 0) | (4 if variant == 1 else 0)
+        h_ = lib().dcl_nlsar_batch_create(n, *args, hs, ws, int(search_window_size), pp, npn, sp, nsn, arr, ns,
+                                          ctypes.c_float(h), ctypes.c_float(c), _mode(select_mode), flags,
+                                          _stream(stream))
+        if not h_:
+            raise DespeckclError(-1, lib().dcl_last_error().decode(errors="replace"))
+        self.handle = h_
+
+    def run(self, stream=None):
+        _check(lib().dcl_nlsar_batch_run(self.handle, _stream(stream)))
+        return self.outs
+
+    @property
+    def variant(self):
+        return lib().dcl_nlsar_batch_variant(self.handle)
+
+    @property
+    def launches(self):
+        return lib().dcl_nlsar_batch_launches(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().dcl_nlsar_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def boxcar_device(a1, a2, phase, window_width, out=None, stream=None):

@@ -51,7 +51,8 @@ struct SceneDesc {
   int vH, vW;      // virtual coordinate whose result lands in row H-1 / column W-1
   int pitch;
   int tiles_x, tiles_y;
-  int tile_begin;  // first global tile index of this scene
+  int tile_begin;  // first launch-wide tile index of this scene
+  int tile_skip;   // scene tiles before the first one this launch covers (chunked scenes)
 };
 
 struct FilterParams {
@@ -127,6 +128,7 @@ cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDes
 // The compile-time specialised kernel (nlsar_fast.cu) for the common
 // configurations; fast_kernel_supported() tells whether `F` has one.
 bool fast_kernel_supported(const FilterParams& F);
-cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st);
+cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
+                              int variant = 0);
 
 }  // namespace dcl

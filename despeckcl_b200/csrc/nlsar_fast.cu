@@ -2,8 +2,8 @@
 // half size and the patch half sizes of a pass (the common configurations),
 // for sm_100a.  Same semantics as the generic kernel in nlsar_kernels.cu.
 //
-// Per CTA: a 32 x 32 output tile, 16 warps, each thread owning 2 vertically
-// consecutive pixels of one column.  For every scale the search-window offsets
+// Per CTA: a 32 x 32 output tile, each thread owning 2 (16 warps) or 4 (8 warps)
+// vertically consecutive pixels of one column.  For every scale the search-window offsets
 // are taken three at a time along a row of the window (same dy, consecutive
 // dx, so a thread's neighbour loads overlap across the batch):
 //   A  GLR similarities of the batch on the tile plus the patch halo
@@ -34,12 +34,12 @@ namespace {
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-template <int WSH, int PH0, int PH1, int PH2>
+template <int WSH, int PH0, int PH1, int PH2, int PX_>
 struct Fast {
   static constexpr int NP = (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
   static constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
   static constexpr int SWS = 2 * WSH + 1;
-  static constexpr int TH = 32, TW = 32, PX = 2;   // 2 vertically adjacent pixels per thread
+  static constexpr int TH = 32, TW = 32, PX = PX_;  // vertically adjacent pixels per thread (2 or 4)
   static constexpr int WARPS = TH / PX, THREADS = 32 * WARPS;
   static constexpr int K = 3;                       // offsets per batch (SWS % K == 0)
   static constexpr int RS = TW + 2 * (PHM + WSH);   // scaled covariance region (square)
@@ -79,10 +79,10 @@ __device__ __forceinline__ constexpr int ph_of(int j) {
   return j == 0 ? PH0 : (j == 1 ? PH1 : PH2);
 }
 
-template <int WSH, int PH0, int PH1, int PH2>
-__global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
+template <int WSH, int PH0, int PH1, int PH2, int PX_>
+__global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
-  using C = Fast<WSH, PH0, PH1, PH2>;
+  using C = Fast<WSH, PH0, PH1, PH2, PX_>;
   constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RO = C::RO;
   constexpr int SIMW = C::SIMW, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
   constexpr int NT = C::THREADS, NW = C::WARPS;
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
       if (scenes[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
     }
     const SceneDesc& S = scenes[lo];
-    const int lt = tile - S.tile_begin;
+    const int lt = tile - S.tile_begin + S.tile_skip;
     const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
     const int vy0 = ty * C::TH, vx0 = tx * TW;
     const int G = P.G, pitch = S.pitch;
@@ -353,19 +353,30 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2>::THREADS, 1)
   }
 }
 
-template <int WSH, int PH0, int PH1, int PH2>
+template <int WSH, int PH0, int PH1, int PH2, int PX_>
 cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
-  using C = Fast<WSH, PH0, PH1, PH2>;
+  using C = Fast<WSH, PH0, PH1, PH2, PX_>;
   const size_t smem = (size_t)C::WORDS * 4;
   static bool configured = false;
   if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(nlsar_fast_kernel<WSH, PH0, PH1, PH2>,
+    const cudaError_t e = cudaFuncSetAttribute(nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  nlsar_fast_kernel<WSH, PH0, PH1, PH2><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
+  nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
   return cudaGetLastError();
+}
+
+template <int PX_>
+cudaError_t launch_fast_px(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
+  const PassParams& p0 = F.pass[0];
+  if (p0.np == 3) return launch_fast_t<10, 1, 2, 3, PX_>(F, d_scenes, grid, st);
+  switch (p0.ph[0]) {
+    case 1: return launch_fast_t<10, 1, -1, -1, PX_>(F, d_scenes, grid, st);
+    case 2: return launch_fast_t<10, 2, -1, -1, PX_>(F, d_scenes, grid, st);
+    default: return launch_fast_t<10, 3, -1, -1, PX_>(F, d_scenes, grid, st);
+  }
 }
 
 }  // namespace
@@ -387,14 +398,12 @@ bool fast_kernel_supported(const FilterParams& F) {
   return false;
 }
 
-cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
-  const PassParams& p0 = F.pass[0];
-  if (p0.np == 3) return launch_fast_t<10, 1, 2, 3>(F, d_scenes, grid, st);
-  switch (p0.ph[0]) {
-    case 1: return launch_fast_t<10, 1, -1, -1>(F, d_scenes, grid, st);
-    case 2: return launch_fast_t<10, 2, -1, -1>(F, d_scenes, grid, st);
-    default: return launch_fast_t<10, 3, -1, -1>(F, d_scenes, grid, st);
-  }
+// variant 0: 2 pixels per thread, 512-thread CTAs (the default); variant 1:
+// 4 pixels per thread, 256-thread CTAs.  The batch autotuner times both.
+cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
+                              int variant) {
+  if (variant == 1) return launch_fast_px<4>(F, d_scenes, grid, st);
+  return launch_fast_px<2>(F, d_scenes, grid, st);
 }
 
 }  // namespace dcl

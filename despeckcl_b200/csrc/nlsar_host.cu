@@ -337,6 +337,10 @@ void profile_count(int n) {
   if (g_prof.on) g_prof.launches += n;
 }
 
+bool uses_specialised_kernel(const Plan& pl) {
+  return !pl.full8 && !g_force_generic && fast_kernel_supported(pl.P);
+}
+
 int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
                 const float* phi, const float* cov_in, cudaStream_t st) {
   dim3 blk(32, 8), grd((g.Wp + 31) / 32, (g.Hp + 7) / 8);
@@ -362,7 +366,8 @@ int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const fl
   return DCL_OK;
 }
 
-int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st) {
+int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st,
+                 int variant) {
   cudaEvent_t a = nullptr, b = nullptr;
   if (g_prof.on) {
     cudaEventCreate(&a);
@@ -370,7 +375,7 @@ int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scene
     cudaEventRecord(a, st);
   }
   const bool fast = !pl.full8 && !g_force_generic && fast_kernel_supported(F);
-  const cudaError_t e = fast ? launch_nlsar_fast(F, d_scenes, F.total_tiles, st)
+  const cudaError_t e = fast ? launch_nlsar_fast(F, d_scenes, F.total_tiles, st, variant)
                              : launch_nlsar_fused(pl.full8, F, d_scenes, smem, F.total_tiles, st);
   if (g_prof.on) {
     cudaEventRecord(b, st);

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (scenes[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
     }
     const SceneDesc& S = scenes[lo];
-    const int lt = tile - S.tile_begin;
+    const int lt = tile - S.tile_begin + S.tile_skip;
     const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
     const int vy0 = ty * TH, vx0 = tx * kTileW;
     const int G = P.G, pitch = S.pitch;

@@ -36,6 +36,10 @@ size_t scratch_bytes(const Plan& pl, const SceneGeom& g);
 void carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d);
 int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
                 const float* phi, const float* cov_in, cudaStream_t st);
-int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st);
+// variant selects the specialised kernel's instantiation (see launch_nlsar_fast)
+int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st,
+                 int variant = 0);
+// whether the call is served by the specialised kernel (variants apply)
+bool uses_specialised_kernel(const Plan& pl);
 
 }  // namespace dcl

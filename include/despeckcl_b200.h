@@ -137,6 +137,33 @@ int dcl_nlsar_insar_batch_device(int n_scenes, const float* const* ampl_master, 
                                  const int* scale_sizes, int n_scale_sizes, const dcl_stats_entry* stats,
                                  int n_stats, float h_param, float c_param, int select_mode, void* stream);
 
+/* Prepared batches.  A batch binds n_scenes device input/output pointer sets
+ * and the filter parameters once: the scratch, the scene descriptors and the
+ * weight tables are set up at creation, every run filters all scenes with one
+ * fused launch.  Flags: DCL_BATCH_GRAPH captures the launch sequence in a CUDA
+ * graph (each run is one graph launch); DCL_BATCH_AUTOTUNE times the
+ * specialised kernel's instantiations on the batch at creation and keeps the
+ * fastest (cached per device and configuration; DESPECKCL_B200_TUNE_CACHE names
+ * a file that keeps the choices across processes); DCL_BATCH_VARIANT1 selects
+ * the 4-pixels-per-thread instantiation without timing.  The batched counterpart of
+ * despeckcl::nlsar (include/despeckcl.h:45-59); the reference filters one scene
+ * per call. */
+enum dcl_batch_flags { DCL_BATCH_GRAPH = 1, DCL_BATCH_AUTOTUNE = 2, DCL_BATCH_VARIANT1 = 4 };
+typedef struct dcl_nlsar_batch dcl_nlsar_batch;
+dcl_nlsar_batch* dcl_nlsar_batch_create(int n_scenes, const float* const* ampl_master,
+                                        const float* const* ampl_slave, const float* const* phase,
+                                        float* const* ref_filt, float* const* phase_filt, float* const* coh_filt,
+                                        const int* heights, const int* widths, int search_window_size,
+                                        const int* patch_sizes, int n_patch_sizes, const int* scale_sizes,
+                                        int n_scale_sizes, const dcl_stats_entry* stats, int n_stats,
+                                        float h_param, float c_param, int select_mode, int flags, void* stream);
+int dcl_nlsar_batch_run(dcl_nlsar_batch* batch, void* stream);
+/* The kernel instantiation in use (0: 2 pixels per thread, 1: 4). */
+int dcl_nlsar_batch_variant(const dcl_nlsar_batch* batch);
+/* Kernels one run launches (prep kernels per scene plus the fused launch). */
+int dcl_nlsar_batch_launches(const dcl_nlsar_batch* batch);
+void dcl_nlsar_batch_destroy(dcl_nlsar_batch* batch);
+
 /* Boxcar filter with a window_width x window_width window; host pointers.
  * Replaces despeckcl::boxcar (include/despeckcl.h:34-43). */
 int dcl_boxcar(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,

@@ -267,3 +267,38 @@ def test_training_matches_oracle(oracle):
         assert a.dissims_max == pytest.approx(b.dissims_max, rel=1e-5)
         assert np.abs(a.quantilles - b.quantilles).max() <= 5.0 / npairs + 1e-7
         np.testing.assert_array_equal(a.chi2cdf_inv, b.chi2cdf_inv)
+
+
+def test_prepared_batch_graph_autotune_equal_single_scenes(train_stats):
+    # a prepared batch (eager, CUDA-graph replay, either kernel instantiation
+    # the autotuner may pick) reproduces the single-scene results bit for bit
+    shapes = [(70, 40), (129, 257), (32, 33), (300, 90)]
+    scenes = [synthetic.insar_scene(h, w, 50 + i) for i, (h, w) in enumerate(shapes)]
+    tens = [tuple(torch.from_numpy(x).cuda() for x in s) for s in scenes]
+    singles = [run_gpu(*s, train_stats, "argmax_enl") for s in scenes]
+    for graph in (False, True):
+        b = dcl.NlsarBatch(tens, SWS, PATCHES, SCALES, train_stats, select_mode="argmax_enl", graph=graph,
+                           autotune=True)
+        assert b.variant in (0, 1)
+        for _ in range(2):
+            outs = b.run()
+            torch.cuda.synchronize()
+            for o, ref in zip(outs, singles):
+                for a, r in zip(o, ref):
+                    np.testing.assert_array_equal(a.cpu().numpy(), r)
+        b.close()
+
+
+def test_kernel_instantiations_agree_bitwise(train_stats):
+    # the 2- and 4-pixel-per-thread instantiations sum in the same per-pixel
+    # order, so they agree exactly
+    a1, a2, ph = synthetic.insar_scene(77, 99, 60)
+    tens = [tuple(torch.from_numpy(x).cuda() for x in (a1, a2, ph))]
+    res = []
+    for v in (0, 1):
+        b = dcl.NlsarBatch(tens, SWS, PATCHES, SCALES, train_stats, graph=False, autotune=False, variant=v)
+        assert b.variant == v
+        res.append([o.cpu().numpy() for o in b.run()[0]])
+        b.close()
+    for a, r in zip(res[0], res[1]):
+        np.testing.assert_array_equal(a, r)
