@@ -48,8 +48,11 @@ def parse():
     p.add_argument("--mode", default="argmax_enl", choices=["argmax_enl", "reference"])
     p.add_argument("--cpu-sample", type=int, default=192, help="side of the CPU-baseline crop")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--config", default="plain", choices=["plain", "batched"],
-                   help="plain: one 4096x4096 scene (the headline); batched: 48 scenes of uneven size")
+    p.add_argument("--config", default="plain", choices=["plain", "batched", "serving"],
+                   help="plain: one 4096x4096 scene (the headline); batched: 48 scenes of uneven size; "
+                        "serving: Poisson request streams through the request server")
+    p.add_argument("--requests", type=int, default=96, help="serving: requests per stream")
+    p.add_argument("--hbm-budget-gb", type=float, default=120.0, help="serving: admission budget")
     return p.parse_args()
 
 
@@ -389,12 +392,151 @@ def run_batched(args):
     return 0
 
 
+def _pct(v, q):
+    import numpy as np
+
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def run_serving(args):
+    """Poisson request streams (0.5, 0.8 and 1.1 times the plain path's
+    request rate) of scenes with sides uniform in [256, 4096], each request
+    seeded by its id, served by the request server (HBM-budget admission,
+    continuous batching) and, under the same arrivals, by the plain path
+    (one scene per call, one call at a time).  Inputs and outputs stay on the
+    device; latency runs from a request's arrival to the end of its last
+    launch."""
+    import threading
+    import time
+
+    import numpy as np
+    import torch
+
+    import despeckcl_b200 as dcl
+    from despeckcl_b200 import synthetic
+
+    torch.cuda.set_device(0)
+    stats = make_stats(dcl, synthetic)
+    n = args.requests
+    rng = np.random.default_rng(5)
+    sizes = [(int(rng.integers(256, 4097)), int(rng.integers(256, 4097))) for _ in range(n)]
+    scenes = [synthetic.insar_scene_device(h, w, i) for i, (h, w) in enumerate(sizes)]
+    outs = [tuple(torch.empty((h, w), device="cuda") for _ in range(3)) for h, w in sizes]
+    torch.cuda.synchronize()
+    px = np.array([h * w for h, w in sizes], dtype=np.float64)
+    stream = torch.cuda.current_stream()
+    kw = dict(select_mode=args.mode)
+
+    def plain_one(i):
+        dcl.nlsar_insar_device(*scenes[i], SWS, PATCHES, SCALES, stats, H_PARAM, C_PARAM, out=outs[i], stream=stream,
+                               **kw)
+
+    # capacities: all requests queued at once
+    for i in range(min(3, n)):
+        plain_one(i)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for i in range(n):
+        plain_one(i)
+        stream.synchronize()
+    t_plain = time.perf_counter() - t
+    mu = n / t_plain
+    budget = int(args.hbm_budget_gb * (1 << 30))
+    srv = dcl.NlsarServer(SWS, PATCHES, SCALES, stats, H_PARAM, C_PARAM, hbm_budget_bytes=budget, **kw)
+    for rid in [srv.submit(*scenes[i], out=outs[i]) for i in range(min(3, n))]:
+        srv.wait(rid, timeout=600)
+    t = time.perf_counter()
+    ids = [srv.submit(*scenes[i], out=outs[i]) for i in range(n)]
+    for rid in ids:
+        srv.wait(rid, timeout=600)
+    t_served = time.perf_counter() - t
+
+    def served_stream(arr):
+        t0 = srv.now() + 0.01
+        ids = [None] * n
+        ready = threading.Semaphore(0)
+
+        def client():
+            for i in range(n):
+                d = t0 + arr[i] - srv.now()
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(*scenes[i], out=outs[i])
+                ready.release()
+
+        th = threading.Thread(target=client)
+        th.start()
+        lat, done, chunks = [], [], []
+        for i in range(n):
+            ready.acquire()
+            _, info = srv.wait(ids[i], timeout=600)
+            lat.append(info["done_s"] - (t0 + arr[i]))
+            done.append(info["done_s"] - t0)
+            chunks.append(info["chunks"])
+        th.join()
+        span = max(done) - arr[0]
+        return {"mpix_s": px.sum() / 1e6 / span, "p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99),
+                "mean_chunks": float(np.mean(chunks))}
+
+    def plain_stream(arr):
+        lat, done = [], []
+        t0 = time.perf_counter() + 0.01
+        for i in range(n):
+            d = t0 + arr[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            plain_one(i)
+            stream.synchronize()
+            e = time.perf_counter() - t0
+            lat.append(e - arr[i])
+            done.append(e)
+        span = max(done) - arr[0]
+        return {"mpix_s": px.sum() / 1e6 / span, "p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99)}
+
+    rates = []
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for k, f in enumerate((0.5, 0.8, 1.1)):
+            lam = f * mu
+            arr = np.cumsum(np.random.default_rng(1000 + k).exponential(1.0 / lam, n))
+            arr -= arr[0]
+            b0 = srv.stats()["batches"]
+            served = served_stream(arr)
+            served["batches"] = srv.stats()["batches"] - b0
+            plain = plain_stream(arr)
+            rates.append({"rate_factor": f, "offered_req_s": lam, "offered_mpix_s": lam * px.mean() / 1e6,
+                          "served": served, "plain": plain})
+    st = srv.stats()
+    srv.close()
+    top = rates[-1]["served"]
+    line = {
+        "metric": "NL-SAR served Mpix/s (Poisson arrivals at 1.1x the plain request rate)",
+        "value": top["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 3,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (generated on the device, seed = request id)",
+        "config": {"workload": f"{n} requests per stream, sides uniform in [256, 4096], "
+                               f"{px.sum() / 1e6:.0f} Mpix per stream",
+                   "search_window": SWS, "patches": PATCHES, "scales": SCALES, "select_mode": args.mode,
+                   "hbm_budget_gb": args.hbm_budget_gb, "max_inflight": 2, "max_batch_tiles": 148 * 8},
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+        "capacity": {"plain_mpix_s": px.sum() / 1e6 / t_plain, "served_mpix_s": px.sum() / 1e6 / t_served,
+                     "plain_req_s": mu, "ratio": t_plain / t_served},
+        "rates": rates,
+        "server": {"batches": st["batches"], "kernel_launches": st["kernel_launches"],
+                   "peak_admitted_gb": st["peak_admitted_bytes"] / 2 ** 30, "peak_inflight": st["peak_inflight"]},
+        "gpu_launches": st["kernel_launches"], "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "batched":
         return run_batched(args)
+    if args.config == "serving":
+        return run_serving(args)
     return run_ours(args)
 
 

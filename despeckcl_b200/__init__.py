@@ -8,6 +8,7 @@ from .api import (  # noqa: F401
     SELECT_MODES,
     DespeckclError,
     NlsarBatch,
+    NlsarServer,
     Params,
     Stats,
     StatsCollection,

@@ -50,6 +50,29 @@ class StatsEntry(ctypes.Structure):
     ]
 
 
+class RequestInfo(ctypes.Structure):
+    """dcl_request_info (include/despeckcl_b200.h)."""
+
+    _fields_ = [("status", ctypes.c_int), ("chunks", ctypes.c_int), ("first_batch", ctypes.c_longlong),
+                ("last_batch", ctypes.c_longlong), ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double),
+                ("launch_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    """dcl_server_stats (include/despeckcl_b200.h)."""
+
+    _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "completed", "failed", "batches", "kernel_launches",
+                                                   "tiles")] + \
+        [(k, ctypes.c_ulonglong) for k in ("budget_bytes", "admitted_bytes", "peak_admitted_bytes")] + \
+        [(k, ctypes.c_int) for k in ("queued", "admitted", "inflight", "peak_inflight")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def lib() -> ctypes.CDLL:
     """The loaded native library (raises if it was not built)."""
     global _LIB
@@ -60,7 +83,8 @@ def lib() -> ctypes.CDLL:
         L.dcl_last_error.restype = ctypes.c_char_p
         L.dcl_version.restype = ctypes.c_char_p
         for fn in ("dcl_nlsar_training_insar", "dcl_nlsar_training_covmat", "dcl_stats_load",
-                   "dcl_stats_collection_from_entries", "dcl_stats_from_dissims", "dcl_nlsar_batch_create"):
+                   "dcl_stats_collection_from_entries", "dcl_stats_from_dissims", "dcl_nlsar_batch_create",
+                   "dcl_server_create"):
             getattr(L, fn).restype = ctypes.c_void_p
         L.dcl_nlsar_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.dcl_nlsar_batch_variant.argtypes = [ctypes.c_void_p]
@@ -71,6 +95,20 @@ def lib() -> ctypes.CDLL:
         L.dcl_stats_collection_free.argtypes = [ctypes.c_void_p]
         L.dcl_stats_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.dcl_stats_load.argtypes = [ctypes.c_char_p]
+        L.dcl_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(StatsEntry),
+                                         ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                         ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.dcl_server_submit.restype = ctypes.c_longlong
+        L.dcl_server_submit.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3 + \
+            [ctypes.c_void_p]
+        L.dcl_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double,
+                                       ctypes.POINTER(RequestInfo)]
+        L.dcl_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(RequestInfo)]
+        L.dcl_server_now.restype = ctypes.c_double
+        L.dcl_server_now.argtypes = [ctypes.c_void_p]
+        L.dcl_server_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
+        L.dcl_server_destroy.argtypes = [ctypes.c_void_p]
         _LIB = L
     return _LIB
 
@@ -391,6 +429,97 @@ class NlsarBatch:
         if getattr(self, "handle", None):
             lib().dcl_nlsar_batch_destroy(self.handle)
             self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NlsarServer:
+    """NL-SAR request server (dcl_server_*): scenes are admitted by a device
+    memory budget and filtered with continuous batching on the current device.
+
+    submit() takes CUDA tensors (read after the work queued so far on the
+    current stream) or numpy arrays (staged through the budget) and returns a
+    request id; wait() returns the request's (ref, phase, coh) and its timing.
+    """
+
+    def __init__(self, search_window_size, patch_sizes, scale_sizes, nlsar_stats, h=15.0, c=49.0,
+                 select_mode="argmax_enl", hbm_budget_bytes=8 << 30, max_inflight=2, max_batch_tiles=148 * 8,
+                 variant=0):
+        pk, pp, npn = _ints(patch_sizes)
+        sk, sp, nsn = _ints(scale_sizes)
+        arr, ns, keep = _entries(nlsar_stats)
+        h_ = lib().dcl_server_create(int(search_window_size), pp, npn, sp, nsn, arr, ns, ctypes.c_float(h),
+                                     ctypes.c_float(c), _mode(select_mode), int(hbm_budget_bytes),
+                                     int(max_inflight), int(max_batch_tiles), 4 if variant == 1 else 0)
+        if not h_:
+            raise DespeckclError(-1, lib().dcl_last_error().decode(errors="replace"))
+        self.handle = h_
+        self._live = {}  # request id -> buffers (and event) kept alive until waited for
+
+    def submit(self, a1, a2, phase, out=None):
+        H, W = a1.shape
+        if isinstance(a1, np.ndarray):
+            ins = tuple(_f32(x) for x in (a1, a2, phase))
+            if out is None:
+                out = tuple(np.empty((H, W), dtype=np.float32) for _ in range(3))
+            ptrs = [ctypes.c_void_p(x.ctypes.data) for x in ins + tuple(out)]
+            host, ev = 1, None
+        else:
+            import torch
+
+            ins = (a1, a2, phase)
+            if out is None:
+                out = tuple(torch.empty((H, W), dtype=torch.float32, device=a1.device) for _ in range(3))
+            ptrs = [_dptr(x) for x in ins + tuple(out)]
+            ev = torch.cuda.Event()
+            ev.record()
+            host = 0
+        rid = lib().dcl_server_submit(self.handle, *ptrs, H, W, host,
+                                      ctypes.c_void_p(ev.cuda_event) if ev is not None else None)
+        if rid < 0:
+            raise DespeckclError(int(rid), lib().dcl_last_error().decode(errors="replace"))
+        self._live[rid] = (ins, out, ev)
+        return rid
+
+    def wait(self, rid, timeout=None):
+        info = RequestInfo()
+        _check(lib().dcl_server_wait(self.handle, rid, -1.0 if timeout is None else float(timeout),
+                                     ctypes.byref(info)))
+        _, out, _ = self._live.pop(rid)
+        if info.status != 0:
+            raise DespeckclError(info.status, f"request {rid} failed: " +
+                                 lib().dcl_last_error().decode(errors="replace"))
+        return out, info.as_dict()
+
+    def poll(self, rid):
+        info = RequestInfo()
+        rc = lib().dcl_server_poll(self.handle, rid, ctypes.byref(info))
+        if rc < 0:
+            _check(rc)
+        if rc == 0:
+            return None
+        _, out, _ = self._live.pop(rid)
+        if info.status != 0:
+            raise DespeckclError(info.status, f"request {rid} failed")
+        return out, info.as_dict()
+
+    def now(self):
+        return lib().dcl_server_now(self.handle)
+
+    def stats(self):
+        s = ServerStats()
+        _check(lib().dcl_server_get_stats(self.handle, ctypes.byref(s)))
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().dcl_server_destroy(self.handle)
+            self.handle = None
+            self._live.clear()
 
     def __del__(self):
         try:

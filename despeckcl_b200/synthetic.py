@@ -75,3 +75,45 @@ def training_area(size: int = 128, seed: int = 7, reflectivity: float = 1.0, coh
     coh = np.full((size, size), coherence, np.float32)
     phase = np.zeros((size, size), np.float32)
     return _speckle(rng, refl, coh, phase)
+
+
+def insar_scene_device(H: int, W: int, seed: int, device="cuda"):
+    """The same recipe drawn with torch's generator on `device`: (ampl_master,
+    ampl_slave, phase) float32 tensors of shape (H, W).  Used where many large
+    scenes are needed quickly (the serving benchmark); the values differ from
+    insar_scene's for the same seed, the distributions do not."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    cpu = np.random.default_rng(seed)
+    refl = torch.full((H, W), float(cpu.lognormal(0.0, 1.0)), device=device)
+    coh = torch.full((H, W), float(cpu.uniform(0.2, 0.95)), device=device)
+    hmin, hmax = math.ceil(H / 16), max(math.ceil(H / 4), math.ceil(H / 16))
+    wmin, wmax = math.ceil(W / 16), max(math.ceil(W / 4), math.ceil(W / 16))
+    for _ in range(40):
+        y0, x0 = int(cpu.integers(0, H)), int(cpu.integers(0, W))
+        hh, ww = int(cpu.integers(hmin, hmax + 1)), int(cpu.integers(wmin, wmax + 1))
+        refl[y0:y0 + hh, x0:x0 + ww] = float(cpu.lognormal(0.0, 1.0))
+        coh[y0:y0 + hh, x0:x0 + ww] = float(cpu.uniform(0.2, 0.95))
+    yy = torch.arange(H, device=device, dtype=torch.float32)[:, None]
+    xx = torch.arange(W, device=device, dtype=torch.float32)[None, :]
+    phase = (2 * math.pi * 3 / W) * xx + torch.zeros_like(yy)
+    for _ in range(5):
+        cy, cx = float(cpu.uniform(0, H)), float(cpu.uniform(0, W))
+        phase = phase + 2 * math.pi * torch.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2 * 30.0 ** 2))
+    phase = torch.atan2(torch.sin(phase), torch.cos(phase))
+
+    def cn():
+        re = torch.randn((H, W), generator=g, device=device)
+        im = torch.randn((H, W), generator=g, device=device)
+        return torch.complex(re, im) * (1 / math.sqrt(2))
+
+    x1, x2 = cn(), cn()
+    l1 = torch.sqrt(refl)
+    l2 = l1 * coh * torch.exp(torch.complex(torch.zeros_like(phase), -phase))
+    l3 = l1 * torch.sqrt(1 - coh * coh)
+    slc1 = l1 * x1
+    slc2 = l2 * x1 + l3 * x2
+    return (slc1.abs().contiguous(), slc2.abs().contiguous(),
+            torch.angle(slc1 * torch.conj(slc2)).float().contiguous())

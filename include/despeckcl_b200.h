@@ -164,6 +164,51 @@ int dcl_nlsar_batch_variant(const dcl_nlsar_batch* batch);
 int dcl_nlsar_batch_launches(const dcl_nlsar_batch* batch);
 void dcl_nlsar_batch_destroy(dcl_nlsar_batch* batch);
 
+/* Request server (no counterpart in the reference, which filters one scene per
+ * blocking call, src/compute/nlsar/nlsar.cpp:139-167).  A server binds the
+ * filter parameters and a device-memory budget on the current device; a worker
+ * thread admits submitted scenes oldest-first while their memory fits the
+ * budget, filters the admitted tiles in launches of at most max_batch_tiles
+ * tiles (large scenes are split over several launches, scenes that arrive while
+ * one runs join the next), and keeps up to max_inflight launches queued on
+ * separate streams.  Results are bitwise those of dcl_nlsar_insar_device on the
+ * same scene.  flags: DCL_BATCH_VARIANT1 as for prepared batches. */
+typedef struct dcl_server dcl_server;
+typedef struct {
+  int status;                  /* DCL_OK, or the error that failed the request */
+  int chunks;                  /* launches the request's tiles were spread over */
+  long long first_batch, last_batch;
+  double submit_s, admit_s, launch_s, done_s; /* seconds since dcl_server_create */
+} dcl_request_info;
+typedef struct {
+  long long submitted, completed, failed, batches, kernel_launches, tiles;
+  unsigned long long budget_bytes, admitted_bytes, peak_admitted_bytes;
+  int queued, admitted, inflight; /* now */
+  int peak_inflight;              /* launches in flight at once, highest seen */
+} dcl_server_stats;
+dcl_server* dcl_server_create(int search_window_size, const int* patch_sizes, int n_patch_sizes,
+                              const int* scale_sizes, int n_scale_sizes, const dcl_stats_entry* stats, int n_stats,
+                              float h_param, float c_param, int select_mode, unsigned long long hbm_budget_bytes,
+                              int max_inflight, int max_batch_tiles, int flags);
+/* Queue one scene.  host_buffers = 0: device pointers, read after
+ * `ready_event` (a cudaEvent_t, or NULL) completes; 1: host pointers (pinned
+ * for overlap), staged through the budget.  Returns the request id (>= 0) or a
+ * negative status (DCL_ERR_OUT_OF_MEMORY when the scene alone exceeds the
+ * budget).  The buffers must stay valid until the request is waited for. */
+long long dcl_server_submit(dcl_server* server, const float* ampl_master, const float* ampl_slave,
+                            const float* phase, float* ref_filt, float* phase_filt, float* coh_filt, int height,
+                            int width, int host_buffers, void* ready_event);
+/* Block until the request has finished (timeout_s < 0: no limit), fill `info`
+ * and forget the request.  Returns DCL_OK when it finished (info->status tells
+ * how), DCL_ERR_TIMEOUT otherwise. */
+int dcl_server_wait(dcl_server* server, long long request, double timeout_s, dcl_request_info* info);
+/* 1 (and `info`, request forgotten) if finished, 0 if not, negative on error. */
+int dcl_server_poll(dcl_server* server, long long request, dcl_request_info* info);
+double dcl_server_now(const dcl_server* server);
+int dcl_server_get_stats(dcl_server* server, dcl_server_stats* out);
+/* Finishes every submitted request, then frees the server. */
+void dcl_server_destroy(dcl_server* server);
+
 /* Boxcar filter with a window_width x window_width window; host pointers.
  * Replaces despeckcl::boxcar (include/despeckcl.h:34-43). */
 int dcl_boxcar(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
