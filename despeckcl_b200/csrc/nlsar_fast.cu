@@ -45,10 +45,14 @@ struct Fast {
   static constexpr int RS = TW + 2 * (PHM + WSH);   // scaled covariance region (square)
   static constexpr int RO = TW + 2 * WSH;           // original covariance region
   static constexpr int SIMW = TW + 2 * PHM;         // similarity region (square)
-  static constexpr int SIMP = SIMW + 1;             // odd pitch: conflict-free row runs
-  static constexpr int HP = TW + 1;                 // horizontal-sum row pitch (words): conflict-free stores
+  // similarity row pitch, a multiple of 8 words: phase A's lanes write
+  // consecutive words; phase B reads 16-byte vectors, a quarter warp covering
+  // 8 consecutive segments of one row (contiguous, conflict free)
+  static constexpr int SIMP = (SIMW + 7) / 8 * 8;
+  static constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
+  static constexpr int HP = TW;                     // horizontal-sum row pitch (words), unpadded
   static constexpr int HPL = K * SIMW * HP;         // one patch size's horizontal-sum plane
-  static constexpr int LUTREP = 8;                  // interleaved LUT copies (bank spread)
+  static constexpr int LUTREP = 16;                 // interleaved LUT copies: two lanes per copy
   // shared memory, in 4-byte words
   static constexpr int OFF_CS = 0;
   static constexpr int OFF_CO = OFF_CS + 4 * RS * RS;
@@ -59,13 +63,19 @@ struct Fast {
   static constexpr int WORDS = OFF_LUT + NP * kMaxLut * LUTREP;
   static_assert(SWS % K == 0, "offset batches must tile a window row");
   static_assert(PH0 >= 0, "at least one patch");
+  static_assert(PX % 2 == 0, "pixels are accumulated in pairs");
+  static_assert(SIMP % 8 == 0 && SIMP >= 4 * 7 + 4 * NQ4, "phase-B segments must stay inside a row");
+  static_assert(HP >= TW && HP % 4 == 0, "horizontal-sum pitch");
+  static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
 };
 
 __device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 b, float lb, float c2d) {
   // sim_measures.h:52-64 with nlooks 1 and the per-pixel ln det precomputed:
   // -(2 d ln 2 + ln det A + ln det B - 2 ln det(A+B)); NaN -> 0.  The two ln det
   // terms are added first, which makes the value exactly symmetric in (A, B).
-  const float s00 = a.x + b.x, s11 = a.y + b.y, sre = a.z + b.z, sim = a.w + b.w;
+  const float2 d01 = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  const float2 d23 = __fadd2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
+  const float s00 = d01.x, s11 = d01.y, sre = d23.x, sim = d23.y;
   const float det = (s00 * s11) - (sre * sre + sim * sim);
   const float t = (la + lb) + c2d;
   float r = fmaf(2.0f * 0.69314718f, __log2f(det), -t);
@@ -116,7 +126,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       sCo[i] = S.cori[(size_t)(vy0 - WSH + r + G) * pitch + (vx0 - WSH + c + G)];
     }
 
-    float acc[PX][NP][8];
+    float2 acc[PX / 2][NP][8];  // .x: pixel 2i, .y: pixel 2i+1
     float best_e[PX], best_a[PX], best_s0[PX], best_m[PX][4];
     int best_rank[PX], best_combo[PX];
 #pragma unroll
@@ -166,11 +176,11 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
 #pragma unroll
       for (int j = 0; j < NP; ++j) lut_j[j] = sLut + j * kMaxLut * C::LUTREP + (lane & (C::LUTREP - 1));
 #pragma unroll
-      for (int i = 0; i < PX; ++i)
+      for (int i = 0; i < PX / 2; ++i)
 #pragma unroll
         for (int j = 0; j < NP; ++j)
 #pragma unroll
-          for (int a = 0; a < 8; ++a) acc[i][j][a] = 0.f;
+          for (int a = 0; a < 8; ++a) acc[i][j][a] = make_float2(0.f, 0.f);
       __syncthreads();
 
       for (int dy = -WSH; dy <= WSH; ++dy) {
@@ -178,10 +188,9 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
           // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
           // thread and consecutive pixels on consecutive lanes (conflict free)
           // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-          constexpr int SIMW8 = (SIMW + 7) / 8 * 8;
-          for (int it = tid; it < SIMW * SIMW8; it += NT) {
-            const int r = it / SIMW8;
-            const int c = it - r * SIMW8;
+          for (int it = tid; it < SIMW * SIMP; it += NT) {
+            const int r = it / SIMP;
+            const int c = it - r * SIMP;
             if (c >= SIMW) continue;
             const int ci = (r + WSH) * RS + (c + WSH);
             const float4 a = sCs[ci];
@@ -192,20 +201,27 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
           }
           __syncthreads();
           // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
-          // quad of rows x 8 column segments; lanes are ordered so that each
-          // quarter warp's float4 stores hit 8 distinct bank groups.
+          // quad of rows x 8 column segments, each quarter warp one row, so its
+          // 16-byte loads and stores are contiguous.
           {
             constexpr int QUADS = (SIMW + 3) / 4;
-            const int r_off = lane & 3;
-            const int seg = ((lane >> 3) << 1) | ((lane >> 2) & 1);
+            const int r_off = lane >> 3;
+            const int seg = lane & 7;
             for (int q = warp; q < K * QUADS; q += NW) {
               const int k = q / QUADS;
               const int r = (q - k * QUADS) * 4 + r_off;
               if (r < SIMW) {
-                const float* row = sSim + (k * SIMW + r) * SIMP + 4 * seg;
-                float s[4 + 2 * PHM];
+                const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMW + r) * SIMP + 4 * seg);
+                float s[4 * C::NQ4];
 #pragma unroll
-                for (int j = 0; j < 4 + 2 * PHM; ++j) s[j] = row[j];
+                for (int q4 = 0; q4 < C::NQ4; ++q4) {
+                  const float4 v = row[q4];
+                  s[4 * q4] = v.x;
+                  s[4 * q4 + 1] = v.y;
+                  s[4 * q4 + 2] = v.z;
+                  s[4 * q4 + 3] = v.w;
+                }
+                float hs[NP][4];
 #pragma unroll
                 for (int o = 0; o < 4; ++o) {
                   float h[3] = {0.f, 0.f, 0.f};
@@ -221,8 +237,12 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
                       if (ph_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
                   }
 #pragma unroll
-                  for (int j = 0; j < NP; ++j) sH[j * C::HPL + (k * SIMW + r) * C::HP + 4 * seg + o] = h[j];
+                  for (int j = 0; j < NP; ++j) hs[j][o] = h[j];
                 }
+#pragma unroll
+                for (int j = 0; j < NP; ++j)
+                  *reinterpret_cast<float4*>(sH + j * C::HPL + (k * SIMW + r) * C::HP + 4 * seg) =
+                      make_float4(hs[j][0], hs[j][1], hs[j][2], hs[j][3]);
               }
             }
           }
@@ -250,9 +270,11 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
               for (int i = 0; i < PX; ++i) {
 #pragma unroll
                 for (int j = 0; j < NP; ++j) {
-                  float d = 0.f;
+                  // top-down sum of the 2ph+1 rows (the first term starts the sum:
+                  // no similarity sum is -0, so this equals 0 + ... bit for bit)
+                  float d = hv[j][i];
 #pragma unroll
-                  for (int a = -ph_of<PH0, PH1, PH2>(j); a <= ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + ph_of<PH0, PH1, PH2>(j) + a];
+                  for (int a = 1; a <= 2 * ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + a];
                   // (unsigned)((clamp(d)-dmin)/(dmax-dmin)*(L-1)) by a saturating
                   // FMA and a round-toward-zero add; d > dmax has weight 0
                   // index = (unsigned)((clamp(d) - dmin) / (dmax - dmin) * (L - 1)):
@@ -267,22 +289,27 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
                 }
               }
             }
+            // two pixels per packed (f32x2) operation; each component is
+            // rounded exactly like the scalar add / multiply / fma
 #pragma unroll
-            for (int i = 0; i < PX; ++i) {
-              const float4 v = sCo[(y0 + i + WSH + dy) * RO + (lane + WSH + dx)];
-              const float x2 = v.x * v.x, y2 = v.y * v.y;
+            for (int i = 0; i < PX; i += 2) {
+              const float4 va = sCo[(y0 + i + WSH + dy) * RO + (lane + WSH + dx)];
+              const float4 vb = sCo[(y0 + i + 1 + WSH + dy) * RO + (lane + WSH + dx)];
+              const float2 vx = make_float2(va.x, vb.x), vy = make_float2(va.y, vb.y);
+              const float2 vz = make_float2(va.z, vb.z), vw = make_float2(va.w, vb.w);
+              const float2 x2 = __fmul2_rn(vx, vx), y2 = __fmul2_rn(vy, vy);
 #pragma unroll
               for (int j = 0; j < NP; ++j) {
-                float* A = acc[i][j];
-                const float ww = w[i][j];
-                A[0] += ww;
-                A[1] = fmaf(ww, ww, A[1]);
-                A[2] = fmaf(ww, v.x, A[2]);
-                A[3] = fmaf(ww, v.y, A[3]);
-                A[4] = fmaf(ww, x2, A[4]);
-                A[5] = fmaf(ww, y2, A[5]);
-                A[6] = fmaf(ww, v.z, A[6]);
-                A[7] = fmaf(ww, v.w, A[7]);
+                float2* A = acc[i / 2][j];
+                const float2 ww = make_float2(w[i][j], w[i + 1][j]);
+                A[0] = __fadd2_rn(A[0], ww);
+                A[1] = __ffma2_rn(ww, ww, A[1]);
+                A[2] = __ffma2_rn(ww, vx, A[2]);
+                A[3] = __ffma2_rn(ww, vy, A[3]);
+                A[4] = __ffma2_rn(ww, x2, A[4]);
+                A[5] = __ffma2_rn(ww, y2, A[5]);
+                A[6] = __ffma2_rn(ww, vz, A[6]);
+                A[7] = __ffma2_rn(ww, vw, A[7]);
               }
             }
           }
@@ -295,7 +322,9 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       for (int i = 0; i < PX; ++i) {
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-          const float* A = acc[i][j];
+          float A[8];
+#pragma unroll
+          for (int a = 0; a < 8; ++a) A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
           const float s0 = A[0], s1 = A[1], s2 = A[2], s3 = A[3], s4 = A[4], s5 = A[5], s6 = A[6], s7 = A[7];
           const float enl = s0 * s0 / s1;
           const float i0 = s2 / s0, i1 = s3 / s0;
