@@ -14,6 +14,8 @@ from .api import (  # noqa: F401
     StatsCollection,
     boxcar,
     boxcar_device,
+    goldstein,
+    goldstein_device,
     lib,
     load_nlsar_stats_collection,
     nlsar,

@@ -317,6 +317,17 @@ def boxcar(ampl_master, ampl_slave, phase, window_width, enabled_log_levels=DEFA
     return ref, phf, coh
 
 
+def goldstein(ampl_master, ampl_slave, phase, patch_size, overlap, alpha, enabled_log_levels=DEFAULT_LOG_LEVELS):
+    """Goldstein filter (swig/python/goldstein.i): returns (reflectivity,
+    phase, coherence); the coherence stays zero as in the reference."""
+    a1, a2, ph = _f32(ampl_master), _f32(ampl_slave), _f32(phase)
+    H, W = _same_shape(a1, a2, ph)
+    ref, phf, coh = (np.zeros((H, W), np.float32) for _ in range(3))
+    _check(lib().dcl_goldstein(_fp(a1), _fp(a2), _fp(ph), _fp(ref), _fp(phf), _fp(coh), H, W, int(patch_size),
+                               int(overlap), ctypes.c_float(alpha)))
+    return ref, phf, coh
+
+
 # ---------------------------------------------------------------------------
 # device entry points (torch CUDA tensors; torch is only the allocator/stream)
 # ---------------------------------------------------------------------------
@@ -526,6 +537,18 @@ class NlsarServer:
             self.close()
         except Exception:
             pass
+
+
+def goldstein_device(a1, a2, phase, patch_size, overlap, alpha, out=None, stream=None):
+    """Goldstein filter on CUDA tensors: fills and returns (ref, phase) tensors."""
+    import torch
+
+    H, W = a1.shape
+    if out is None:
+        out = tuple(torch.empty((H, W), dtype=torch.float32, device=a1.device) for _ in range(2))
+    _check(lib().dcl_goldstein_device(_dptr(a1), _dptr(a2), _dptr(phase), _dptr(out[0]), _dptr(out[1]), None, H, W,
+                                      int(patch_size), int(overlap), ctypes.c_float(alpha), _stream(stream)))
+    return out
 
 
 def boxcar_device(a1, a2, phase, window_width, out=None, stream=None):

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/despeckcl_b200.h"
+#include "dcl_internal.h"
 #include "stats_internal.h"
 
 namespace {
@@ -107,6 +108,19 @@ int despeckcl::boxcar(float* a1, float* a2, float* phi, float* ref, float* phase
   const Logger log(levels);
   const auto t0 = std::chrono::steady_clock::now();
   return finish(log, dcl_boxcar(a1, a2, phi, ref, phase, coh, height, width, window_width), "boxcar", t0);
+}
+
+int despeckcl::goldstein(float* a1, float* a2, float* phi, float* ref, float* phase, float* coh,
+                         const unsigned int height, const unsigned int width, const unsigned int patch_size,
+                         const unsigned int overlap, const float alpha, std::vector<std::string> levels) {
+  const Logger log(levels);
+  const auto t0 = std::chrono::steady_clock::now();
+  if (height > 0x7fffffffu || width > 0x7fffffffu || patch_size > 0x7fffffffu || overlap > 0x7fffffffu)
+    return finish(log, dcl::set_error(DCL_ERR_INVALID_ARGUMENT, "dimensions out of range"), "goldstein", t0);
+  return finish(log,
+                dcl_goldstein(a1, a2, phi, ref, phase, coh, (int)height, (int)width, (int)patch_size, (int)overlap,
+                              alpha),
+                "goldstein", t0);
 }
 
 int despeckcl::nlsar(float* a1, float* a2, float* phi, float* ref, float* phase, float* coh, const int height,

@@ -1,0 +1,364 @@
+// Goldstein phase filter of an InSAR pair (despeckcl::goldstein,
+// src/compute/goldstein/goldstein.cpp:39-106 and
+// goldstein_filter_sub_image.cpp:27-187 in the reference), for 32 x 32
+// patches.
+//
+// The reference cuts the scene into tiles of side
+//   sub = round_up(max(H, W) + 2 ov, s),  s = p - 2 ov,  round_up(n, m) = n - n % m + m
+// (goldstein.cpp:62-65, tile_size.cpp:27-36; that side whenever it fits its
+// device allocation bound, i.e. every scene up to tens of thousands of pixels
+// a side), at origins -ov + k (sub - 2 ov) while below H / W
+// (tile_iterator.cpp), and writes each tile's centre back with clamping, later
+// tiles over earlier ones (map_filter_tiles.h:64-96, sub_images.cpp:47-69).
+// The result at (y, x) is therefore tile row y / (sub - 2 ov) at tile row
+// y - origin for y < H-1, and the last tile row at tile row sub - ov - 1 for
+// y = H-1 (columns alike).  Per tile, only the patches behind those final
+// positions are filtered.  Two kernels per tile:
+//
+//  goldstein_patch_kernel  one warp per patch: gathers the 32 x 32 patch of the
+//     clamp-extended raw interferogram Z = 0.5 (a1 + a2) e^{j phi}
+//     (raw_interferogram.cl, patches_unpack.cl, sub_images.cpp), transforms it
+//     with a 2-D FFT (rows then columns, each a 32-point radix-2 FFT held in a
+//     lane's registers, shared memory for the transposes), multiplies by
+//     |Z|^alpha (weighted_multiply.cl), transforms back with the 1/p^2 scale
+//     of the reference's clFFT plan (goldstein_patch_ft_test.cpp) and stores the
+//     patch;
+//  goldstein_pack_kernel   one thread per output pixel: the raw interferogram
+//     plus the weighted contributions of the (up to four) patches covering the
+//     pixel, added in the order of the reference's four parity launches, which
+//     accumulate onto the buffer that still holds the raw interferogram
+//     (patches_pack.cl:29-71, patches_pack.cpp:48-77); then |Z| and arg Z
+//     (slc2real.cl).  Output row H-1 (column W-1) takes the last tile row
+//     (column) of the clamped write-back (sub_images.cpp:47-69).
+// The coherence output is not written, as in the reference.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/despeckcl_b200.h"
+#include "dcl_internal.h"
+
+namespace dcl {
+namespace {
+
+constexpr int kP = 32;           // patch side (the FFT length)
+constexpr int kWarps = 4;        // patches per CTA (34 KB of transpose buffers)
+constexpr int kPitch = kP + 1;   // float2 row pitch of a warp's transpose buffer
+
+// W_32^m = exp(-2 pi i m / 32), m = 0..15
+__constant__ float2 c_tw32[16] = {
+    {1.000000000e+00f, -0.000000000e+00f}, {9.807852804e-01f, -1.950903220e-01f},
+    {9.238795325e-01f, -3.826834324e-01f}, {8.314696123e-01f, -5.555702330e-01f},
+    {7.071067812e-01f, -7.071067812e-01f}, {5.555702330e-01f, -8.314696123e-01f},
+    {3.826834324e-01f, -9.238795325e-01f}, {1.950903220e-01f, -9.807852804e-01f},
+    {0.000000000e+00f, -1.000000000e+00f}, {-1.950903220e-01f, -9.807852804e-01f},
+    {-3.826834324e-01f, -9.238795325e-01f}, {-5.555702330e-01f, -8.314696123e-01f},
+    {-7.071067812e-01f, -7.071067812e-01f}, {-8.314696123e-01f, -5.555702330e-01f},
+    {-9.238795325e-01f, -3.826834324e-01f}, {-9.807852804e-01f, -1.950903220e-01f},
+};
+
+__host__ __device__ constexpr int rev5(int i) {
+  return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
+}
+
+// In-register 32-point radix-2 decimation-in-time FFT (forward: e^{-i}, no
+// scaling; inverse: e^{+i}, no scaling).
+template <bool INV>
+__device__ __forceinline__ void fft32(float2 (&x)[kP]) {
+#pragma unroll
+  for (int i = 0; i < kP; ++i) {
+    const int j = rev5(i);
+    if (j > i) {
+      const float2 t = x[i];
+      x[i] = x[j];
+      x[j] = t;
+    }
+  }
+#pragma unroll
+  for (int half = 1; half < kP; half <<= 1) {
+#pragma unroll
+    for (int i = 0; i < kP; i += 2 * half) {
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        const int m = k * (kP / (2 * half));  // twiddle index into W_32
+        const float2 a = x[i + k];
+        const float2 b = x[i + k + half];
+        float2 t;
+        if (m == 0) {
+          t = b;
+        } else if (m == 8) {  // W = -i (forward), +i (inverse)
+          t = INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+        } else {
+          const float2 w = c_tw32[m];
+          const float wy = INV ? -w.y : w.y;
+          t = make_float2(b.x * w.x - b.y * wy, b.x * wy + b.y * w.x);
+        }
+        x[i + k] = make_float2(a.x + t.x, a.y + t.y);
+        x[i + k + half] = make_float2(a.x - t.x, a.y - t.y);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int clampg(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+struct GoldsteinGeom {
+  int H, W, ov, s, sub, n;
+};
+
+// One tile of the reference's tiling and the part of it this call computes.
+struct GoldsteinTile {
+  int h0, w0;          // image position of tile pixel (0, 0)
+  int py_lo, px_lo;    // first patch row / column filtered
+  int n_py, n_px;      // patches filtered per column / row
+  int y_lo, y_hi;      // output rows whose final value comes from this tile (inclusive)
+  int x_lo, x_hi;      // output columns likewise
+};
+
+__global__ void __launch_bounds__(32 * kWarps)
+    goldstein_patch_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
+                           float2* __restrict__ patches, GoldsteinGeom g, GoldsteinTile t, float alpha) {
+  __shared__ float2 sbuf[kWarps][kP * kPitch];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pid = blockIdx.x * kWarps + warp;
+  if (pid >= t.n_py * t.n_px) return;  // whole warp leaves together
+  float2* buf = sbuf[warp];
+  const int py = t.py_lo + pid / t.n_px, px = t.px_lo + pid % t.n_px;
+  // gather: lane = column of the patch
+  {
+    const int tx = clampg(px * g.s + lane - g.ov, 0, g.sub - 1);
+    const int ix = clampg(t.w0 + tx, 0, g.W - 1);
+#pragma unroll 4
+    for (int r = 0; r < kP; ++r) {
+      const int ty = clampg(py * g.s + r - g.ov, 0, g.sub - 1);
+      const int iy = clampg(t.h0 + ty, 0, g.H - 1);
+      const size_t i = (size_t)iy * g.W + ix;
+      const float amp = 0.5f * (a1[i] + a2[i]);
+      float sn, cs;
+      sincosf(phi[i], &sn, &cs);
+      buf[r * kPitch + lane] = make_float2(amp * cs, amp * sn);
+    }
+  }
+  __syncwarp();
+  float2 x[kP];
+  // rows (lane = row), forward
+#pragma unroll
+  for (int k = 0; k < kP; ++k) x[k] = buf[lane * kPitch + k];
+  fft32<false>(x);
+#pragma unroll
+  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = x[k];
+  __syncwarp();
+  // columns (lane = column): forward, |Z|^alpha weight, inverse
+#pragma unroll
+  for (int r = 0; r < kP; ++r) x[r] = buf[r * kPitch + lane];
+  fft32<false>(x);
+#pragma unroll
+  for (int r = 0; r < kP; ++r) {
+    const float psd = sqrtf(x[r].x * x[r].x + x[r].y * x[r].y);
+    const float w = powf(psd, alpha);
+    x[r] = make_float2(w * x[r].x, w * x[r].y);
+  }
+  fft32<true>(x);
+#pragma unroll
+  for (int r = 0; r < kP; ++r) buf[r * kPitch + lane] = x[r];
+  __syncwarp();
+  // rows, inverse, scaled by 1/p^2 (a power of two: exact)
+#pragma unroll
+  for (int k = 0; k < kP; ++k) x[k] = buf[lane * kPitch + k];
+  fft32<true>(x);
+  constexpr float kScale = 1.0f / (kP * kP);
+#pragma unroll
+  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = make_float2(x[k].x * kScale, x[k].y * kScale);
+  __syncwarp();
+  float2* out = patches + (size_t)pid * kP * kP;
+#pragma unroll 4
+  for (int r = 0; r < kP; ++r) out[r * kP + lane] = buf[r * kPitch + lane];
+}
+
+// weight of a patch sample in the overlap-add (patches_pack.cl:50-63)
+__device__ __forceinline__ float pack_factor(int rel, int o, int ov, int sub) {
+  float f = 1.0f;
+  if (rel < 2 * ov || rel >= kP - 2 * ov) f *= 0.5f;
+  if (o < ov || o >= sub - ov) f *= 2.0f;
+  return f;
+}
+
+__global__ void __launch_bounds__(256)
+    goldstein_pack_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
+                          const float2* __restrict__ patches, float* __restrict__ ref, float* __restrict__ phase,
+                          GoldsteinGeom g, GoldsteinTile t) {
+  const int x = t.x_lo + blockIdx.x * 32 + (threadIdx.x & 31);
+  const int y = t.y_lo + blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (x > t.x_hi || y > t.y_hi) return;
+  // tile position whose result lands here (the clamped write-back keeps the
+  // last one; only the last tile row / column reaches row H-1 / column W-1)
+  const int ty = (y == g.H - 1) ? g.sub - g.ov - 1 : y - t.h0;
+  const int tx = (x == g.W - 1) ? g.sub - g.ov - 1 : x - t.w0;
+  float2 v;
+  {
+    const size_t i = (size_t)clampg(t.h0 + ty, 0, g.H - 1) * g.W + clampg(t.w0 + tx, 0, g.W - 1);
+    const float amp = 0.5f * (a1[i] + a2[i]);
+    float sn, cs;
+    sincosf(phi[i], &sn, &cs);
+    v = make_float2(amp * cs, amp * sn);
+  }
+  // covering patches per axis: q = (t + ov) / s at offset t + ov - q s, and
+  // q - 1 at offset + s when that is still inside the patch (one of each parity)
+  const int qx = (tx + g.ov) / g.s, cx = tx + g.ov - qx * g.s;
+  const int qy = (ty + g.ov) / g.s, ry = ty + g.ov - qy * g.s;
+  const int pxa[2] = {qx, qx - 1}, cxa[2] = {cx, cx + g.s};
+  const bool vxa[2] = {qx >= t.px_lo && qx < t.px_lo + t.n_px,
+                       qx - 1 >= t.px_lo && qx - 1 < t.px_lo + t.n_px && cx + g.s < kP};
+  const int pya[2] = {qy, qy - 1}, rya[2] = {ry, ry + g.s};
+  const bool vya[2] = {qy >= t.py_lo && qy < t.py_lo + t.n_py,
+                       qy - 1 >= t.py_lo && qy - 1 < t.py_lo + t.n_py && ry + g.s < kP};
+  // launch order: (x parity, y parity) = (0,0), (0,1), (1,0), (1,1)
+#pragma unroll
+  for (int xpar = 0; xpar < 2; ++xpar)
+#pragma unroll
+    for (int ypar = 0; ypar < 2; ++ypar)
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          if (!vxa[a] || !vya[b] || (pxa[a] & 1) != xpar || (pya[b] & 1) != ypar) continue;
+          const float f = pack_factor(cxa[a], tx, g.ov, g.sub) * pack_factor(rya[b], ty, g.ov, g.sub);
+          const float2 q =
+              patches[((size_t)(pya[b] - t.py_lo) * t.n_px + (pxa[a] - t.px_lo)) * kP * kP + rya[b] * kP + cxa[a]];
+          v.x += f * q.x;
+          v.y += f * q.y;
+        }
+  const size_t o = (size_t)y * g.W + x;
+  ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
+  phase[o] = atan2f(v.y, v.x);
+}
+
+// patches (of the n per side) covering tile positions [lo, hi]
+void patch_span(const GoldsteinGeom& g, int lo, int hi, int& first, int& count) {
+  // patch q covers [q s - ov, q s - ov + p)
+  int a = lo + g.ov - kP + 1;
+  a = a <= 0 ? 0 : (a + g.s - 1) / g.s;
+  int b = (hi + g.ov) / g.s;
+  if (b > g.n - 1) b = g.n - 1;
+  first = a;
+  count = b - a + 1;
+}
+
+}  // namespace
+
+int goldstein_geom(int H, int W, int p, int ov, GoldsteinGeom& g) {
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  if (p != kP) return set_error(DCL_ERR_UNSUPPORTED, "patch size %d: the GPU Goldstein filter supports 32", p);
+  if (ov < 0 || kP - 2 * ov <= 2 * ov)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "overlap must satisfy 0 <= overlap < patch_size / 4, got %d", ov);
+  g.H = H;
+  g.W = W;
+  g.ov = ov;
+  g.s = kP - 2 * ov;
+  const long long m = (long long)std::max(H, W) + 2 * ov;
+  const long long sub = m - m % g.s + g.s;
+  if (sub > (1 << 20)) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
+  g.sub = (int)sub;
+  g.n = g.sub / g.s;
+  return DCL_OK;
+}
+
+// The reference's tiles (tile_iterator.cpp with tile side g.sub and overlap
+// ov) and, per tile, the output rectangle it finally owns and the patches
+// behind it.
+std::vector<GoldsteinTile> goldstein_tiles(const GoldsteinGeom& g) {
+  const int step = g.sub - 2 * g.ov;
+  std::vector<int> h0s, w0s;
+  for (int h0 = -g.ov; h0 < g.H; h0 += step) h0s.push_back(h0);
+  for (int w0 = -g.ov; w0 < g.W; w0 += step) w0s.push_back(w0);
+  std::vector<GoldsteinTile> tiles;
+  for (size_t i = 0; i < h0s.size(); ++i)
+    for (size_t j = 0; j < w0s.size(); ++j) {
+      GoldsteinTile t;
+      t.h0 = h0s[i];
+      t.w0 = w0s[j];
+      const bool last_r = i + 1 == h0s.size(), last_c = j + 1 == w0s.size();
+      // rows [i step, (i+1) step) below H-1, plus row H-1 for the last tile row
+      t.y_lo = std::min((int)i * step, g.H - 1);
+      t.y_hi = last_r ? g.H - 1 : std::min(((int)i + 1) * step, g.H - 1) - 1;
+      t.x_lo = std::min((int)j * step, g.W - 1);
+      t.x_hi = last_c ? g.W - 1 : std::min(((int)j + 1) * step, g.W - 1) - 1;
+      // tile positions read: y - h0 for y < H-1, sub - ov - 1 for y = H-1
+      const int ty_lo = (t.y_lo < g.H - 1) ? t.y_lo - t.h0 : g.sub - g.ov - 1;
+      const int ty_hi = last_r ? g.sub - g.ov - 1 : t.y_hi - t.h0;
+      const int tx_lo = (t.x_lo < g.W - 1) ? t.x_lo - t.w0 : g.sub - g.ov - 1;
+      const int tx_hi = last_c ? g.sub - g.ov - 1 : t.x_hi - t.w0;
+      patch_span(g, ty_lo, ty_hi, t.py_lo, t.n_py);
+      patch_span(g, tx_lo, tx_hi, t.px_lo, t.n_px);
+      tiles.push_back(t);
+    }
+  return tiles;
+}
+
+int goldstein_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase, int H, int W, int p,
+                     int ov, float alpha, cudaStream_t st) {
+  if (!a1 || !a2 || !phi || !ref || !phase) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  GoldsteinGeom g;
+  int rc = goldstein_geom(H, W, p, ov, g);
+  if (rc) return rc;
+  const std::vector<GoldsteinTile> tiles = goldstein_tiles(g);
+  size_t np = 0;
+  for (const GoldsteinTile& t : tiles) np = std::max(np, (size_t)t.n_py * t.n_px);
+  float2* patches = nullptr;
+  cudaError_t e = cudaMallocAsync(&patches, np * kP * kP * sizeof(float2), st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(Goldstein patches)");
+  // tiles in the reference's order; each pack writes only the pixels its tile
+  // owns, so one patch buffer serves the tiles in turn
+  for (const GoldsteinTile& t : tiles) {
+    const size_t n = (size_t)t.n_py * t.n_px;
+    goldstein_patch_kernel<<<(unsigned)((n + kWarps - 1) / kWarps), 32 * kWarps, 0, st>>>(a1, a2, phi, patches, g, t,
+                                                                                         alpha);
+    dim3 grid((t.x_hi - t.x_lo + 32) / 32, (t.y_hi - t.y_lo + 8) / 8);
+    goldstein_pack_kernel<<<grid, 256, 0, st>>>(a1, a2, phi, patches, ref, phase, g, t);
+  }
+  e = cudaGetLastError();
+  cudaFreeAsync(patches, st);
+  if (e != cudaSuccess) return cuda_error(e, "Goldstein launch");
+  return DCL_OK;
+}
+
+}  // namespace dcl
+
+extern "C" int dcl_goldstein_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+                                    float* coh, int H, int W, int patch_size, int overlap, float alpha, void* stream) {
+  (void)coh;  // not written (slc2real.cl writes amplitude and phase only)
+  return dcl::goldstein_device(a1, a2, phi, ref, phase, H, W, patch_size, overlap, alpha, (cudaStream_t)stream);
+}
+
+extern "C" int dcl_goldstein(const float* a1, const float* a2, const float* phi, float* ref, float* phase, float* coh,
+                             int H, int W, int patch_size, int overlap, float alpha) {
+  (void)coh;
+  if (!a1 || !a2 || !phi || !ref || !phase) return dcl::set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  dcl::GoldsteinGeom g;
+  const int vr = dcl::goldstein_geom(H, W, patch_size, overlap, g);
+  if (vr) return vr;
+  cudaStream_t st = cudaStreamPerThread;
+  const size_t n = (size_t)H * W, b = n * sizeof(float);
+  float* buf = nullptr;
+  cudaError_t e = cudaMallocAsync(&buf, 5 * b, st);
+  if (e != cudaSuccess) return dcl::cuda_error(e, "cudaMallocAsync(Goldstein)");
+  e = cudaMemcpyAsync(buf, a1, b, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n, a2, b, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 2 * n, phi, b, cudaMemcpyHostToDevice, st);
+  int rc = DCL_OK;
+  if (e != cudaSuccess) rc = dcl::cuda_error(e, "cudaMemcpyAsync(H2D)");
+  if (rc == DCL_OK)
+    rc = dcl::goldstein_device(buf, buf + n, buf + 2 * n, buf + 3 * n, buf + 4 * n, H, W, patch_size, overlap, alpha,
+                               st);
+  if (rc == DCL_OK) {
+    e = cudaMemcpyAsync(ref, buf + 3 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(phase, buf + 4 * n, b, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = dcl::cuda_error(e, "cudaMemcpyAsync(D2H)");
+  }
+  cudaFreeAsync(buf, st);
+  e = cudaStreamSynchronize(st);
+  if (rc == DCL_OK && e != cudaSuccess) rc = dcl::cuda_error(e, "Goldstein");
+  return rc;
+}

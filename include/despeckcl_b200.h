@@ -18,6 +18,8 @@
  *                                                                          src/compute/nlsar/training/nlsar_training.cpp:99-113
  *   dcl_boxcar*              despeckcl::boxcar(...)                      include/despeckcl.h:34-43,
  *                                                                          src/compute/boxcar/boxcar.cpp:30-100
+ *   dcl_goldstein*           despeckcl::goldstein(...)                   include/despeckcl.h:111-122,
+ *                                                                          src/compute/goldstein/goldstein.cpp:39-106
  *   dcl_stats_entry          nlsar::params + nlsar::stats                include/compute/nlsar/parameters.h:26-57,
  *                                                                          include/compute/nlsar/stats.h:28-55
  */
@@ -218,6 +220,23 @@ int dcl_boxcar(const float* ampl_master, const float* ampl_slave, const float* p
  * despeckcl::boxcar (include/despeckcl.h:34-43). */
 int dcl_boxcar_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
                       float* phase_filt, float* coh_filt, int height, int width, int window_width, void* stream);
+
+/* Goldstein phase filter with patch_size x patch_size FFT patches (32 on the
+ * GPU), overlap `overlap` and exponent `alpha`; host pointers.  ref_filt gets
+ * the filtered interferogram's amplitude and phase_filt its phase; coh_filt is
+ * not written (the reference leaves it as passed).  Scenes are one tile of the
+ * reference's tiling, which holds for every scene whose padded side fits the
+ * reference's device allocation bound.  Replaces despeckcl::goldstein
+ * (include/despeckcl.h:111-122). */
+int dcl_goldstein(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                  float* phase_filt, float* coh_filt, int height, int width, int patch_size, int overlap,
+                  float alpha);
+
+/* Same on device pointers, asynchronous on `stream`.  Replaces
+ * despeckcl::goldstein (include/despeckcl.h:111-122). */
+int dcl_goldstein_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                         float* phase_filt, float* coh_filt, int height, int width, int patch_size, int overlap,
+                         float alpha, void* stream);
 
 /* Training on a homogeneous area; host pointers.  Returns NULL on failure.
  * Replaces despeckcl::nlsar_training (include/despeckcl.h:75-83). */

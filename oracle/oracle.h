@@ -38,6 +38,11 @@ int oracle_nlsar_training_insar(const float* a1, const float* a2, const float* p
                                 int* out_scale, float* out_dmin, float* out_dmax, float* out_quant,
                                 float* out_chi2);
 
+// Goldstein filter, one tile (goldstein_oracle.cpp)
+int oracle_goldstein(const float* a1, const float* a2, const float* phi, float* ref, float* phase, int H, int W,
+                     int patch_size, int overlap, float alpha, int use_double);
+int oracle_goldstein_tile_side(int H, int W, int patch_size, int overlap);
+
 #ifdef __cplusplus
 }
 #endif

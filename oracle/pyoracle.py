@@ -271,3 +271,34 @@ def boxcar(a1, a2, phi, window_width, tile=512):
     if rc != 0:
         raise RuntimeError(f"oracle_boxcar failed: {rc}")
     return ref, ph, coh
+
+
+def goldstein(a1, a2, phi, patch_size=32, overlap=4, alpha=0.5, use_double=True):
+    """Goldstein filter restatement (goldstein_oracle.cpp): (ref, phase)."""
+    a1, a2, phi = _f32(a1), _f32(a2), _f32(phi)
+    H, W = a1.shape
+    ref = np.zeros((H, W), np.float32)
+    ph = np.zeros((H, W), np.float32)
+    rc = lib().oracle_goldstein(_fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), H, W, int(patch_size), int(overlap),
+                                ctypes.c_float(alpha), int(bool(use_double)))
+    if rc:
+        raise ValueError("unsupported Goldstein parameters")
+    return ref, ph
+
+
+def ref_goldstein(a1, a2, phi, patch_size=32, overlap=4, alpha=0.5, coh=None):
+    """The reference's own Goldstein kernels run on the CPU (oracle/_ref):
+    (ref, phase, coh), or None when they were not built here."""
+    R = ref_pieces()
+    if R is None:
+        return None
+    a1, a2, phi = _f32(a1), _f32(a2), _f32(phi)
+    H, W = a1.shape
+    ref = np.zeros((H, W), np.float32)
+    ph = np.zeros((H, W), np.float32)
+    c = np.zeros((H, W), np.float32) if coh is None else _f32(coh).copy()
+    rc = R.ref_goldstein(_fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), _fp(c), H, W, int(patch_size),
+                         int(overlap), ctypes.c_float(alpha))
+    if rc:
+        raise ValueError("scene smaller than two patches per side")
+    return ref, ph, c
