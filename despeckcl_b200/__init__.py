@@ -22,6 +22,8 @@ from .api import (  # noqa: F401
     nlsar_insar,
     nlsar_insar_batch_device,
     nlsar_insar_device,
+    nlinsar,
+    nlinsar_device,
     nlsar_train,
     nlsar_train_insar,
     store_nlsar_stats_collection,

@@ -328,6 +328,18 @@ def goldstein(ampl_master, ampl_slave, phase, patch_size, overlap, alpha, enable
     return ref, phf, coh
 
 
+def nlinsar(ampl_master, ampl_slave, phase, search_window_size, patch_size, niter, lmin,
+            enabled_log_levels=DEFAULT_LOG_LEVELS):
+    """NL-InSAR filter (swig/python/nlinsar.i): returns (reflectivity, phase,
+    coherence), starting from zero estimates as the reference's binding does."""
+    a1, a2, ph = _f32(ampl_master), _f32(ampl_slave), _f32(phase)
+    H, W = _same_shape(a1, a2, ph)
+    ref, phf, coh = (np.zeros((H, W), np.float32) for _ in range(3))
+    _check(lib().dcl_nlinsar(_fp(a1), _fp(a2), _fp(ph), _fp(ref), _fp(phf), _fp(coh), H, W, int(search_window_size),
+                             int(patch_size), int(niter), int(lmin)))
+    return ref, phf, coh
+
+
 # ---------------------------------------------------------------------------
 # device entry points (torch CUDA tensors; torch is only the allocator/stream)
 # ---------------------------------------------------------------------------
@@ -537,6 +549,20 @@ class NlsarServer:
             self.close()
         except Exception:
             pass
+
+
+def nlinsar_device(a1, a2, phase, search_window_size, patch_size, niter, lmin, estimates=None, stream=None):
+    """NL-InSAR on CUDA tensors: `estimates` = (ref, phase, coh) tensors with
+    the initial estimates (zeros when omitted), overwritten with the results."""
+    import torch
+
+    H, W = a1.shape
+    if estimates is None:
+        estimates = tuple(torch.zeros((H, W), dtype=torch.float32, device=a1.device) for _ in range(3))
+    _check(lib().dcl_nlinsar_device(_dptr(a1), _dptr(a2), _dptr(phase), _dptr(estimates[0]), _dptr(estimates[1]),
+                                    _dptr(estimates[2]), H, W, int(search_window_size), int(patch_size), int(niter),
+                                    int(lmin), _stream(stream)))
+    return estimates
 
 
 def goldstein_device(a1, a2, phase, patch_size, overlap, alpha, out=None, stream=None):

@@ -21,6 +21,9 @@ OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(PKG, "libdespeckcl_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
+# per-file flags: NL-InSAR rounds every product and sum separately, like the
+# reference's kernels (no multiply-add contraction)
+FILE_FLAGS = {"nlinsar.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -42,7 +45,7 @@ def _deps_newer(src: str, obj: str) -> bool:
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
     if _deps_newer(src, obj):
-        cmd = [nvcc()] + ARCH + FLAGS + ["-c", src, "-o", obj]
+        cmd = [nvcc()] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

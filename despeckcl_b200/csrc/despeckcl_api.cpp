@@ -110,6 +110,16 @@ int despeckcl::boxcar(float* a1, float* a2, float* phi, float* ref, float* phase
   return finish(log, dcl_boxcar(a1, a2, phi, ref, phase, coh, height, width, window_width), "boxcar", t0);
 }
 
+int despeckcl::nlinsar(float* a1, float* a2, float* phi, float* ref, float* phase, float* coh, const int height,
+                       const int width, const int search_window_size, const int patch_size, const int niter,
+                       const int lmin, std::vector<std::string> levels) {
+  const Logger log(levels);
+  const auto t0 = std::chrono::steady_clock::now();
+  return finish(log,
+                dcl_nlinsar(a1, a2, phi, ref, phase, coh, height, width, search_window_size, patch_size, niter, lmin),
+                "nlinsar", t0);
+}
+
 int despeckcl::goldstein(float* a1, float* a2, float* phi, float* ref, float* phase, float* coh,
                          const unsigned int height, const unsigned int width, const unsigned int patch_size,
                          const unsigned int overlap, const float alpha, std::vector<std::string> levels) {

@@ -2,7 +2,7 @@
  *
  * Same declarations as the reference's include/despeckcl.h:30-95 for the
  * functions implemented here (nlsar x2, nlsar_training x2,
- * store/load_nlsar_stats_collection, boxcar, goldstein).  Every function returns 0 on
+ * store/load_nlsar_stats_collection, boxcar, goldstein, nlinsar).  Every function returns 0 on
  * success like the reference; on failure it returns the negative dcl_status of
  * despeckcl_b200.h (the reference terminates the process instead) and logs the
  * message at the "error" level.
@@ -26,6 +26,10 @@ typedef std::map<nlsar::params, nlsar::stats> nlsar_stats_collection;
 namespace despeckcl {
 int boxcar(float* ampl_master, float* ampl_slave, float* phase, float* ref_filt, float* phase_filt, float* coh_filt,
            const int height, const int width, const int window_width, std::vector<std::string> enabled_log_levels);
+
+int nlinsar(float* ampl_master, float* ampl_slave, float* phase, float* ref_filt, float* phase_filt, float* coh_filt,
+            const int height, const int width, const int search_window_size, const int patch_size, const int niter,
+            const int lmin, std::vector<std::string> enabled_log_levels);
 
 int goldstein(float* ampl_master, float* ampl_slave, float* phase, float* ref_filt, float* phase_filt,
               float* coh_filt, const unsigned int height, const unsigned int width, const unsigned int patch_size,

@@ -20,6 +20,8 @@
  *                                                                          src/compute/boxcar/boxcar.cpp:30-100
  *   dcl_goldstein*           despeckcl::goldstein(...)                   include/despeckcl.h:111-122,
  *                                                                          src/compute/goldstein/goldstein.cpp:39-106
+ *   dcl_nlinsar*             despeckcl::nlinsar(...)                     include/despeckcl.h:97-109,
+ *                                                                          src/compute/nlinsar/nlinsar.cpp:42-130
  *   dcl_stats_entry          nlsar::params + nlsar::stats                include/compute/nlsar/parameters.h:26-57,
  *                                                                          include/compute/nlsar/stats.h:28-55
  */
@@ -237,6 +239,22 @@ int dcl_goldstein(const float* ampl_master, const float* ampl_slave, const float
 int dcl_goldstein_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
                          float* phase_filt, float* coh_filt, int height, int width, int patch_size, int overlap,
                          float alpha, void* stream);
+
+/* NL-InSAR with a search window search_window_size^2, patch_size^2 patches
+ * (3 or 7: the sizes for which the reference tabulates its h), niter passes
+ * and at least lmin looks (1..64); host pointers.  ref_filt, phase_filt and
+ * coh_filt hold the initial estimates on entry (the Python binding passes
+ * zeros) and the results on exit.  Replaces despeckcl::nlinsar
+ * (include/despeckcl.h:97-109). */
+int dcl_nlinsar(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                float* phase_filt, float* coh_filt, int height, int width, int search_window_size, int patch_size,
+                int niter, int lmin);
+
+/* Same on device pointers, asynchronous on `stream`.  Replaces
+ * despeckcl::nlinsar (include/despeckcl.h:97-109). */
+int dcl_nlinsar_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
+                       float* phase_filt, float* coh_filt, int height, int width, int search_window_size,
+                       int patch_size, int niter, int lmin, void* stream);
 
 /* Training on a homogeneous area; host pointers.  Returns NULL on failure.
  * Replaces despeckcl::nlsar_training (include/despeckcl.h:75-83). */

@@ -43,6 +43,11 @@ int oracle_goldstein(const float* a1, const float* a2, const float* phi, float* 
                      int patch_size, int overlap, float alpha, int use_double);
 int oracle_goldstein_tile_side(int H, int W, int patch_size, int overlap);
 
+// NL-InSAR (nlinsar_oracle.cpp)
+float oracle_nlinsar_h_theo(int patch_size);
+int oracle_nlinsar(const float* a1, const float* a2, const float* ph, float* ref, float* phase, float* coh, int H,
+                   int W, int sws, int patch_size, int niter, int lmin, int use_double, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -302,3 +302,39 @@ def ref_goldstein(a1, a2, phi, patch_size=32, overlap=4, alpha=0.5, coh=None):
     if rc:
         raise ValueError("scene smaller than two patches per side")
     return ref, ph, c
+
+
+def nlinsar(a1, a2, phi, sws=21, patch_size=7, niter=5, lmin=10, use_double=True, init=None, threads=0):
+    """NL-InSAR restatement (nlinsar_oracle.cpp): (ref, phase, coh); the
+    initial estimates are zeros (as the Python binding passes) unless given."""
+    a1, a2, phi = _f32(a1), _f32(a2), _f32(phi)
+    H, W = a1.shape
+    if init is None:
+        ref, ph, coh = (np.zeros((H, W), np.float32) for _ in range(3))
+    else:
+        ref, ph, coh = (_f32(x).copy() for x in init)
+    rc = lib().oracle_nlinsar(_fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), _fp(coh), H, W, int(sws),
+                              int(patch_size), int(niter), int(lmin), int(bool(use_double)),
+                              int(threads or os.cpu_count() or 1))
+    if rc:
+        raise ValueError("unsupported NL-InSAR parameters")
+    return ref, ph, coh
+
+
+def ref_nlinsar(a1, a2, phi, sws=21, patch_size=7, niter=5, lmin=10, init=None):
+    """The reference's own NL-InSAR pieces run on the CPU (oracle/_ref), or
+    None when they were not built here."""
+    R = ref_pieces()
+    if R is None:
+        return None
+    a1, a2, phi = _f32(a1), _f32(a2), _f32(phi)
+    H, W = a1.shape
+    if init is None:
+        ref, ph, coh = (np.zeros((H, W), np.float32) for _ in range(3))
+    else:
+        ref, ph, coh = (_f32(x).copy() for x in init)
+    rc = R.ref_nlinsar(_fp(a1), _fp(a2), _fp(phi), _fp(ref), _fp(ph), _fp(coh), H, W, int(sws), int(patch_size),
+                       int(niter), int(lmin))
+    if rc:
+        raise ValueError("unsupported NL-InSAR parameters")
+    return ref, ph, coh
