@@ -46,11 +46,14 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=4096)
     p.add_argument("--mode", default="argmax_enl", choices=["argmax_enl", "reference"])
-    p.add_argument("--cpu-sample", type=int, default=192, help="side of the CPU-baseline crop")
+    p.add_argument("--cpu-sample", type=int, default=704,
+                   help="side of the CPU-baseline crop (about 10 s of oracle work on 16 host cores)")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--config", default="plain", choices=["plain", "batched", "serving"],
+    p.add_argument("--config", default="plain", choices=["plain", "batched", "serving", "secondary"],
                    help="plain: one 4096x4096 scene (the headline); batched: 48 scenes of uneven size; "
-                        "serving: Poisson request streams through the request server")
+                        "serving: Poisson request streams through the request server; secondary: Goldstein, "
+                        "boxcar and NL-InSAR on an 8192x8192 scene")
+    p.add_argument("--nlinsar-size", type=int, default=2048, help="secondary: side of the NL-InSAR scene")
     p.add_argument("--requests", type=int, default=96, help="serving: requests per stream")
     p.add_argument("--hbm-budget-gb", type=float, default=120.0, help="serving: admission budget")
     return p.parse_args()
@@ -529,6 +532,78 @@ def run_serving(args):
     return 0
 
 
+def run_secondary(args):
+    """The secondary filters on the precision-study scene (8192 x 8192 by
+    default, --size): Goldstein (patch 32, overlap 4, alpha 0.5), boxcar
+    (window 7) and NL-InSAR (search 21, patch 7, lmin 10; one pass per step,
+    --nlinsar-size scene).  Each is timed with CUDA events on the launching
+    stream over K steps with inputs resident in HBM, larger than L2."""
+    import torch
+
+    import despeckcl_b200 as dcl
+    from despeckcl_b200 import synthetic
+
+    torch.cuda.set_device(0)
+    L = dcl.lib()
+    stream = torch.cuda.current_stream()
+    S = args.size if args.size != 4096 else 8192
+    a1, a2, ph = synthetic.insar_scene_device(S, S, 4)
+    k = max(1, args.steps)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        L.dcl_profile_begin()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        import ctypes
+        n_all = ctypes.c_long()
+        L.dcl_profile_end(None, None, ctypes.byref(n_all))
+        return a.elapsed_time(b) / k, int(n_all.value)
+
+    hbm = None
+    try:
+        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        hbm, hbm_src = 6650.0, "fallback 6.65 TB/s"
+    res = {}
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        g_out = tuple(torch.empty((S, S), device="cuda") for _ in range(2))
+        ms, n = timed(lambda: dcl.goldstein_device(a1, a2, ph, 32, 4, 0.5, out=g_out, stream=stream))
+        # algorithmic bytes: three planes in, reflectivity and phase out
+        res["goldstein"] = {"mpix_s": S * S / (ms * 1e-3) / 1e6, "ms": ms, "launches_per_step": n / k,
+                            "roofline": {"bound": "hbm", "bytes_per_pixel": 20,
+                                         "achieved_gbs": 20 * S * S / (ms * 1e-3) / 1e9, "peak_gbs": hbm,
+                                         "frac": 20 * S * S / (ms * 1e-3) / 1e9 / hbm}}
+        b_out = tuple(torch.empty((S, S), device="cuda") for _ in range(3))
+        ms, n = timed(lambda: dcl.boxcar_device(a1, a2, ph, 7, out=b_out, stream=stream))
+        res["boxcar"] = {"mpix_s": S * S / (ms * 1e-3) / 1e6, "ms": ms, "launches_per_step": n / k,
+                         "roofline": {"bound": "hbm", "bytes_per_pixel": 24,
+                                      "achieved_gbs": 24 * S * S / (ms * 1e-3) / 1e9, "peak_gbs": hbm,
+                                      "frac": 24 * S * S / (ms * 1e-3) / 1e9 / hbm}}
+        Sn = min(args.nlinsar_size, S)
+        n1, n2, nph = (x[:Sn, :Sn].contiguous() for x in (a1, a2, ph))
+        est = tuple(torch.zeros((Sn, Sn), device="cuda") for _ in range(3))
+        ms, n = timed(lambda: dcl.nlinsar_device(n1, n2, nph, 21, 7, 1, 10, estimates=est, stream=stream))
+        res["nlinsar"] = {"mpix_s_per_pass": Sn * Sn / (ms * 1e-3) / 1e6, "ms_per_pass": ms, "side": Sn,
+                          "launches_per_step": n / k}
+    line = {"metric": "secondary filters Mpix/s", "value": res["goldstein"]["mpix_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": k, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (generated on the device, seed 4)",
+            "config": {"workload": f"{S}x{S} scene: Goldstein p32 ov4 a0.5, boxcar w7, NL-InSAR sws21 p7 lmin10 "
+                                   f"one pass on {min(args.nlinsar_size, S)}^2",
+                       "l2": f"inputs {3 * S * S * 4 / 1e6:.0f} MB > L2 126 MB"},
+            "hbm_peak_source": hbm_src, "filters": res, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -537,6 +612,8 @@ def main():
         return run_batched(args)
     if args.config == "serving":
         return run_serving(args)
+    if args.config == "secondary":
+        return run_secondary(args)
     return run_ours(args)
 
 

@@ -109,6 +109,7 @@ int boxcar_device(const float* a1, const float* a2, const float* phi, float* ref
     configured = smem;
   }
   boxcar_kernel<<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W, r);
+  profile_count(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "boxcar launch");
   return DCL_OK;

@@ -317,6 +317,7 @@ int goldstein_device(const float* a1, const float* a2, const float* phi, float* 
                                                                                          alpha);
     dim3 grid((t.x_hi - t.x_lo + 32) / 32, (t.y_hi - t.y_lo + 8) / 8);
     goldstein_pack_kernel<<<grid, 256, 0, st>>>(a1, a2, phi, patches, ref, phase, g, t);
+    profile_count(2);
   }
   e = cudaGetLastError();
   cudaFreeAsync(patches, st);

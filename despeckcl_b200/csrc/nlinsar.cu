@@ -394,6 +394,7 @@ int nlinsar_device(const float* a1, const float* a2, const float* dp, float* ref
   e = cudaFuncSetAttribute(nlinsar_weights_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
     nlinsar_filter_values_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a1, a2, dp, fa, fr, fi, n);
+    profile_count(1);
     // estimates ping-pong between the caller's planes and tr/tp/tc; an odd
     // number of passes ends in tr/tp/tc and is copied back
     float* cur[3] = {ref, phase, coh};
@@ -405,6 +406,7 @@ int nlinsar_device(const float* a1, const float* a2, const float* dp, float* ref
         dim3 grid((unsigned)((npix + kEstThreads - 1) / kEstThreads), nt);
         nlinsar_estimate_kernel<<<grid, kEstThreads, 0, st>>>(a1, fa, fr, fi, cur[0], cur[1], cur[2], nxt[0], nxt[1],
                                                               nxt[2], g, t0, wts, nols);
+        profile_count(2);
       }
       std::swap(cur, nxt);
     }
