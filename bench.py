@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--size", type=int, default=4096)
+    p.add_argument("--size", type=int, default=None, help="scene side (plain: 4096, secondary: 8192)")
     p.add_argument("--mode", default="argmax_enl", choices=["argmax_enl", "reference"])
     p.add_argument("--cpu-sample", type=int, default=704,
                    help="side of the CPU-baseline crop (about 10 s of oracle work on 16 host cores)")
@@ -546,7 +546,7 @@ def run_secondary(args):
     torch.cuda.set_device(0)
     L = dcl.lib()
     stream = torch.cuda.current_stream()
-    S = args.size if args.size != 4096 else 8192
+    S = args.size or 8192
     a1, a2, ph = synthetic.insar_scene_device(S, S, 4)
     k = max(1, args.steps)
 
@@ -606,6 +606,8 @@ def run_secondary(args):
 
 def main():
     args = parse()
+    if args.size is None and args.config != "secondary":
+        args.size = 4096
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "batched":

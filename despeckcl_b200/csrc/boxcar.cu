@@ -22,7 +22,7 @@ namespace dcl {
 namespace {
 
 constexpr int kBoxTW = 64;
-constexpr int kBoxTH = 16;
+constexpr int kBoxTH = 32;
 constexpr int kBoxThreads = 256;
 constexpr int kBoxMaxR = 15;
 
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kBoxThreads)
     const size_t g = (size_t)y * W + x;
     const float am = a1[g], as = a2[g];
     float sn, cs;
-    sincosf(phi[g], &sn, &cs);
+    __sincosf(phi[g], &sn, &cs);
     const float aa = am * as;
     sI[i] = (am * am + as * as) / 2;
     sR[i] = aa * cs;

@@ -102,11 +102,26 @@ __device__ __forceinline__ void fft32(float2 (&x)[kP]) {
   }
 }
 
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ int clampg(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 struct GoldsteinGeom {
   int H, W, ov, s, sub, n;
+  float inv_s;  // 1 / s
 };
+
+// n / s for 0 <= n < 2^24: a float estimate corrected to the exact quotient
+__device__ __forceinline__ int div_s(int n, const GoldsteinGeom& g) {
+  int q = __float2int_rz((float)n * g.inv_s);
+  if (q * g.s > n) --q;
+  if ((q + 1) * g.s <= n) ++q;
+  return q;
+}
 
 // One tile of the reference's tiling and the part of it this call computes.
 struct GoldsteinTile {
@@ -137,7 +152,7 @@ __global__ void __launch_bounds__(32 * kWarps)
       const size_t i = (size_t)iy * g.W + ix;
       const float amp = 0.5f * (a1[i] + a2[i]);
       float sn, cs;
-      sincosf(phi[i], &sn, &cs);
+      __sincosf(phi[i], &sn, &cs);
       buf[r * kPitch + lane] = make_float2(amp * cs, amp * sn);
     }
   }
@@ -154,10 +169,12 @@ __global__ void __launch_bounds__(32 * kWarps)
 #pragma unroll
   for (int r = 0; r < kP; ++r) x[r] = buf[r * kPitch + lane];
   fft32<false>(x);
+  // |Z|^alpha = 2^(alpha/2 log2 |Z|^2) (pow(0, 0) = 1 kept for alpha = 0)
+  const float half_alpha = 0.5f * alpha;
 #pragma unroll
   for (int r = 0; r < kP; ++r) {
-    const float psd = sqrtf(x[r].x * x[r].x + x[r].y * x[r].y);
-    const float w = powf(psd, alpha);
+    const float m2 = x[r].x * x[r].x + x[r].y * x[r].y;
+    const float w = (alpha == 0.0f) ? 1.0f : ex2_approx(half_alpha * __log2f(m2));
     x[r] = make_float2(w * x[r].x, w * x[r].y);
   }
   fft32<true>(x);
@@ -201,35 +218,52 @@ __global__ void __launch_bounds__(256)
     const size_t i = (size_t)clampg(t.h0 + ty, 0, g.H - 1) * g.W + clampg(t.w0 + tx, 0, g.W - 1);
     const float amp = 0.5f * (a1[i] + a2[i]);
     float sn, cs;
-    sincosf(phi[i], &sn, &cs);
+    __sincosf(phi[i], &sn, &cs);
     v = make_float2(amp * cs, amp * sn);
   }
   // covering patches per axis: q = (t + ov) / s at offset t + ov - q s, and
   // q - 1 at offset + s when that is still inside the patch (one of each parity)
-  const int qx = (tx + g.ov) / g.s, cx = tx + g.ov - qx * g.s;
-  const int qy = (ty + g.ov) / g.s, ry = ty + g.ov - qy * g.s;
-  const int pxa[2] = {qx, qx - 1}, cxa[2] = {cx, cx + g.s};
-  const bool vxa[2] = {qx >= t.px_lo && qx < t.px_lo + t.n_px,
-                       qx - 1 >= t.px_lo && qx - 1 < t.px_lo + t.n_px && cx + g.s < kP};
-  const int pya[2] = {qy, qy - 1}, rya[2] = {ry, ry + g.s};
-  const bool vya[2] = {qy >= t.py_lo && qy < t.py_lo + t.n_py,
-                       qy - 1 >= t.py_lo && qy - 1 < t.py_lo + t.n_py && ry + g.s < kP};
-  // launch order: (x parity, y parity) = (0,0), (0,1), (1,0), (1,1)
+  const int qx = div_s(tx + g.ov, g), cx = tx + g.ov - qx * g.s;
+  const int qy = div_s(ty + g.ov, g), ry = ty + g.ov - qy * g.s;
+  // candidate 0: patch q, candidate 1: patch q - 1; e = the even one
+  const bool vx0 = qx >= t.px_lo && qx < t.px_lo + t.n_px;
+  const bool vx1 = qx - 1 >= t.px_lo && qx - 1 < t.px_lo + t.n_px && cx + g.s < kP;
+  const bool vy0 = qy >= t.py_lo && qy < t.py_lo + t.n_py;
+  const bool vy1 = qy - 1 >= t.py_lo && qy - 1 < t.py_lo + t.n_py && ry + g.s < kP;
+  const bool xe1 = qx & 1, ye1 = qy & 1;  // the even patch is candidate 1
+  int px_[2], cx_[2], py_[2], ry_[2];
+  bool vx_[2], vy_[2];
+  float fx_[2], fy_[2];
+  // index 0: even parity, 1: odd parity
+  px_[0] = xe1 ? qx - 1 : qx;
+  px_[1] = xe1 ? qx : qx - 1;
+  cx_[0] = xe1 ? cx + g.s : cx;
+  cx_[1] = xe1 ? cx : cx + g.s;
+  vx_[0] = xe1 ? vx1 : vx0;
+  vx_[1] = xe1 ? vx0 : vx1;
+  py_[0] = ye1 ? qy - 1 : qy;
+  py_[1] = ye1 ? qy : qy - 1;
+  ry_[0] = ye1 ? ry + g.s : ry;
+  ry_[1] = ye1 ? ry : ry + g.s;
+  vy_[0] = ye1 ? vy1 : vy0;
+  vy_[1] = ye1 ? vy0 : vy1;
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    fx_[a] = pack_factor(cx_[a], tx, g.ov, g.sub);
+    fy_[a] = pack_factor(ry_[a], ty, g.ov, g.sub);
+  }
+  // the reference's four parity launches in order: (x, y) parity (0,0), (0,1), (1,0), (1,1)
 #pragma unroll
   for (int xpar = 0; xpar < 2; ++xpar)
 #pragma unroll
-    for (int ypar = 0; ypar < 2; ++ypar)
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          if (!vxa[a] || !vya[b] || (pxa[a] & 1) != xpar || (pya[b] & 1) != ypar) continue;
-          const float f = pack_factor(cxa[a], tx, g.ov, g.sub) * pack_factor(rya[b], ty, g.ov, g.sub);
-          const float2 q =
-              patches[((size_t)(pya[b] - t.py_lo) * t.n_px + (pxa[a] - t.px_lo)) * kP * kP + rya[b] * kP + cxa[a]];
-          v.x += f * q.x;
-          v.y += f * q.y;
-        }
+    for (int ypar = 0; ypar < 2; ++ypar) {
+      if (!vx_[xpar] || !vy_[ypar]) continue;
+      const float f = fx_[xpar] * fy_[ypar];
+      const float2 q = patches[((size_t)(py_[ypar] - t.py_lo) * t.n_px + (px_[xpar] - t.px_lo)) * kP * kP +
+                               ry_[ypar] * kP + cx_[xpar]];
+      v.x += f * q.x;
+      v.y += f * q.y;
+    }
   const size_t o = (size_t)y * g.W + x;
   ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
   phase[o] = atan2f(v.y, v.x);
@@ -257,6 +291,7 @@ int goldstein_geom(int H, int W, int p, int ov, GoldsteinGeom& g) {
   g.W = W;
   g.ov = ov;
   g.s = kP - 2 * ov;
+  g.inv_s = 1.0f / (float)g.s;
   const long long m = (long long)std::max(H, W) + 2 * ov;
   const long long sub = m - m % g.s + g.s;
   if (sub > (1 << 20)) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
@@ -302,6 +337,9 @@ int goldstein_device(const float* a1, const float* a2, const float* phi, float* 
   if (!a1 || !a2 || !phi || !ref || !phase) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   GoldsteinGeom g;
   int rc = goldstein_geom(H, W, p, ov, g);
+  if (rc) return rc;
+  int dev = 0;
+  rc = ensure_device_ready(dev);
   if (rc) return rc;
   const std::vector<GoldsteinTile> tiles = goldstein_tiles(g);
   size_t np = 0;

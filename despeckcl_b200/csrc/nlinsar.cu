@@ -375,6 +375,11 @@ int nlinsar_device(const float* a1, const float* a2, const float* dp, float* ref
                    int W, int sws, int p, int niter, int lmin, cudaStream_t st) {
   if (!a1 || !a2 || !dp || !ref || !phase || !coh) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   if (niter < 0) return set_error(DCL_ERR_INVALID_ARGUMENT, "niter must be >= 0");
+  {
+    int dev = 0;
+    const int rc0 = ensure_device_ready(dev);
+    if (rc0) return rc0;
+  }
   NlGeom g;
   int rc = nlinsar_geom(H, W, sws, p, lmin, g);
   if (rc) return rc;

@@ -140,6 +140,17 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       for (int d = 0; d < 4; ++d) best_m[i][d] = 0.f;
     }
 
+    // phase-A items of this thread (fixed for the whole launch): the
+    // similarity-map position it = tid + m NT, as an index into the scaled
+    // covariance region, or -1 past the map or in a row's padding
+    constexpr int A_ITEMS = (SIMW * SIMP + NT - 1) / NT;
+    int a_ci[A_ITEMS];
+#pragma unroll
+    for (int m = 0; m < A_ITEMS; ++m) {
+      const int it = tid + m * NT;
+      const int r = it / SIMP, c = it - (it / SIMP) * SIMP;
+      a_ci[m] = (it < SIMW * SIMP && c < SIMW) ? (r + WSH) * RS + (c + WSH) : -1;
+    }
     int loaded_slot = -1;
     for (int ps = 0; ps < P.npass; ++ps) {
       const PassParams& pp = P.pass[ps];
@@ -188,16 +199,16 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
           // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
           // thread and consecutive pixels on consecutive lanes (conflict free)
           // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-          for (int it = tid; it < SIMW * SIMP; it += NT) {
-            const int r = it / SIMP;
-            const int c = it - r * SIMP;
-            if (c >= SIMW) continue;
-            const int ci = (r + WSH) * RS + (c + WSH);
+#pragma unroll
+          for (int m = 0; m < A_ITEMS; ++m) {
+            const int it = tid + m * NT;
+            const int ci = a_ci[m];
+            if (ci < 0) continue;
             const float4 a = sCs[ci];
             const float la = sLd[ci];
             const int ni = ci + dy * RS + dx0;
 #pragma unroll
-            for (int k = 0; k < K; ++k) sSim[(k * SIMW + r) * SIMP + c] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
+            for (int k = 0; k < K; ++k) sSim[k * SIMW * SIMP + it] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
           }
           __syncthreads();
           // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
@@ -313,7 +324,10 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
               }
             }
           }
-          __syncthreads();
+          // no barrier here: the next batch's phase A writes only the
+          // similarity map, which every warp finished reading (phase B)
+          // before the barrier above; its barrier after phase A orders this
+          // phase C's reads of the horizontal sums before they are rewritten
         }
       }
 

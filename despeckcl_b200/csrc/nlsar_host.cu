@@ -232,7 +232,7 @@ int make_plan(int sws, const int* patches, int np, const int* scales, int ns, co
 static std::mutex g_init_mu;
 static bool g_pool_ready[64];
 
-static int ensure_device_ready(int& dev) {
+int ensure_device_ready(int& dev) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
   std::lock_guard<std::mutex> lk(g_init_mu);
