@@ -74,6 +74,28 @@ template <typename T> inline T det2(T e00, T e01r, T e01i, T e11) {
 }
 
 template <typename T>
+inline T det3(T a00, T a11, T a22, T a01r, T a01i, T a02r, T a02i, T a12r, T a12i) {
+  // sim_measures.h:66-97 (Leibniz formula of a Hermitian 3x3 matrix)
+  return a00 * a11 * a22 - a00 * (a12r * a12r + a12i * a12i) - a11 * (a02r * a02r + a02i * a02i) -
+         a22 * (a01r * a01r + a01i * a01i) +
+         2 * (a01r * a12r * a02r - a01i * a12i * a02r + a01r * a12i * a02i + a01i * a12r * a02i);
+}
+
+// Pixel similarity of two Hermitian 3x3 matrices given by their 9 unique
+// reals {a00, a11, a22, Re a01, Im a01, Re a02, Im a02, Re a12, Im a12}
+// (sim_measures.h:100-160, nlooks = 1, dimensions = 3).
+template <typename T> inline T glr_3x3(const T* a, const T* b) {
+  const T nom1 = det3<T>(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]);
+  const T nom2 = det3<T>(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8]);
+  const T det = det3<T>(a[0] + b[0], a[1] + b[1], a[2] + b[2], a[3] + b[3], a[4] + b[4], a[5] + b[5], a[6] + b[6],
+                        a[7] + b[7], a[8] + b[8]);
+  const T two = T(2);
+  T sim = -T(1) * (T(2 * 3) * std::log(two) + std::log(nom1) + std::log(nom2) - two * std::log(det));
+  if (std::isnan(sim)) sim = T(0);
+  return sim;
+}
+
+template <typename T>
 inline T glr_2x2(T a00, T a01r, T a01i, T a11, T b00, T b01r, T b01i, T b11) {
   // sim_measures.h:37-65, nlooks = 1, dimensions = 2
   const T nom1 = det2<T>(a00, a01r, a01i, a11);
@@ -86,16 +108,35 @@ inline T glr_2x2(T a00, T a01r, T a01i, T a11, T b00, T b01r, T b01i, T b11) {
   return sim;
 }
 
-// A covariance tile: 8 planes [2*d*d][h][w], even planes real, odd imaginary
+// A covariance tile: 2*d*d planes [2*d*d][h][w] (d = 2 or 3), plane
+// 2*(r*d+c) the real and 2*(r*d+c)+1 the imaginary part of element (r, c)
 // (covmat_create.cl:44-54 layout).
 template <typename T> struct Cov {
-  int h = 0, w = 0;
+  int h = 0, w = 0, d = 2, np = 8;
   std::vector<T> v;
   Cov() = default;
-  Cov(int hh, int ww) : h(hh), w(ww), v((size_t)8 * hh * ww) {}
+  Cov(int hh, int ww, int dd = 2) : h(hh), w(ww), d(dd), np(2 * dd * dd), v((size_t)2 * dd * dd * hh * ww) {}
   T& at(int plane, int y, int x) { return v[((size_t)plane * h + y) * w + x]; }
   T at(int plane, int y, int x) const { return v[((size_t)plane * h + y) * w + x]; }
+  // real plane of element (r, c)
+  int plane(int r, int c) const { return 2 * (r * d + c); }
 };
+
+// Pixel similarity of the covariance at (ay, ax) of `ca` and (by, bx) of `cb`
+// (compute_pixel_similarities_{2x2,3x3}.cl.in: upper-triangle planes only).
+template <typename T> T glr_at(const Cov<T>& ca, int ay, int ax, const Cov<T>& cb, int by, int bx) {
+  if (ca.d == 2)
+    return glr_2x2<T>(ca.at(0, ay, ax), ca.at(2, ay, ax), ca.at(3, ay, ax), ca.at(6, ay, ax), cb.at(0, by, bx),
+                      cb.at(2, by, bx), cb.at(3, by, bx), cb.at(6, by, bx));
+  // a00, a11, a22, a01, a02, a12 (planes 0, 8, 16, 2/3, 4/5, 10/11)
+  static const int pl[9] = {0, 8, 16, 2, 3, 4, 5, 10, 11};
+  T a[9], b[9];
+  for (int i = 0; i < 9; ++i) {
+    a[i] = ca.at(pl[i], ay, ax);
+    b[i] = cb.at(pl[i], by, bx);
+  }
+  return glr_3x3<T>(a, b);
+}
 
 // ---------------------------------------------------------------------------
 // stages
@@ -125,18 +166,22 @@ Cov<T> covmat_create(const float* a1, const float* a2, const float* ph, int h, i
   return c;
 }
 
-template <typename T> T rescale_gamma() {
-  // covmat_rescale.cl:25-26 with nlooks = 1, dimension = 2
-  const T LD = T(1) / T(2);
+template <typename T> T rescale_gamma(int dim = 2) {
+  // covmat_rescale.cl:25-26 with nlooks = 1
+  const T LD = T(1) / T(dim);
   return std::pow(std::min(LD, T(1)), T(0.33333f));
 }
 
 template <typename T> void covmat_rescale(Cov<T>& c) {
-  // covmat_rescale.cl:31-39: every off-diagonal plane (2,3,4,5) times gamma
-  const T g = rescale_gamma<T>();
-  for (int pl = 2; pl <= 5; ++pl)
-    for (int y = 0; y < c.h; ++y)
-      for (int x = 0; x < c.w; ++x) c.at(pl, y, x) *= g;
+  // covmat_rescale.cl:31-39: both planes of every off-diagonal element times gamma
+  const T g = rescale_gamma<T>(c.d);
+  for (int r = 0; r < c.d; ++r)
+    for (int col = 0; col < c.d; ++col) {
+      if (r == col) continue;
+      for (int pl = c.plane(r, col); pl <= c.plane(r, col) + 1; ++pl)
+        for (int y = 0; y < c.h; ++y)
+          for (int x = 0; x < c.w; ++x) c.at(pl, y, x) *= g;
+    }
 }
 
 template <typename T> std::vector<T> gen_gauss(int s) {
@@ -161,8 +206,8 @@ template <typename T> Cov<T> covmat_spatial_avg(const Cov<T>& in, int s, int sma
   const int delta = (smax - s) / 2;
   const int ho = in.h - smax + 1, wo = in.w - smax + 1;
   const std::vector<T> g = gen_gauss<T>(s);
-  Cov<T> out(ho, wo);
-  for (int pl = 0; pl < 8; ++pl)
+  Cov<T> out(ho, wo, in.d);
+  for (int pl = 0; pl < in.np; ++pl)
     for (int y = 0; y < ho; ++y)
       for (int x = 0; x < wo; ++x) {
         T sum = T(0);
@@ -177,7 +222,7 @@ template <typename T> Cov<T> covmat_spatial_avg(const Cov<T>& in, int s, int sma
 // Per-combination results for one tile core.
 template <typename T> struct ComboResult {
   std::vector<T> enl_nobias, alpha, wsum;
-  std::vector<T> mean8;       // 8 planes of sum(w*C)/sum(w) over the core
+  std::vector<T> mean8;       // every plane's sum(w*C) over the core
   std::vector<T> bin_margin;  // FP64 diagnostics: min distance of a LUT index to a bin edge
   std::vector<T> var_cond;    // FP64 diagnostics: min over d of |var_d| / I_d^2 (alpha conditioning)
   std::vector<T> kappa;       // FP64 diagnostics: sum w|C01| / |sum w C01| (cancellation in the complex mean)
@@ -239,7 +284,7 @@ struct FilterParams {
 // Output of one tile: 8 filtered planes on the core plus diagnostics.
 template <typename T> struct TileOut {
   int hc = 0, wc = 0;
-  std::vector<T> cov8;       // [8][hc][wc]
+  std::vector<T> cov8;       // [2*d*d][hc][wc]
   std::vector<int> sel;      // selected combo index (loop order: scale outer, patch inner)
   std::vector<T> bin_margin, enl_margin, var_cond, kappa, bin_margin_all;
 };
@@ -291,9 +336,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
               const int cy = y + wsh, cx = x;
               const int wy = cy - wsh + hh, wx = cx - wsh + ww;
               if (wx < 0 || wx >= Wo) continue;  // never read downstream
-              pix[((size_t)(hh * sws + ww) * Hsym + y) * Wo + x] =
-                  glr_2x2<T>(cs.at(0, cy, cx), cs.at(2, cy, cx), cs.at(3, cy, cx), cs.at(6, cy, cx),
-                             cs.at(0, wy, wx), cs.at(2, wy, wx), cs.at(3, wy, wx), cs.at(6, wy, wx));
+              pix[((size_t)(hh * sws + ww) * Hsym + y) * Wo + x] = glr_at<T>(cs, cy, cx, cs, wy, wx);
             }
     };
     quadrant(0, wsh, wsh, sws, 0);        // first quadrant, offset {0,0}
@@ -354,7 +397,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
       R.enl_nobias.assign(nc, 0);
       R.alpha.assign(nc, 0);
       R.wsum.assign(nc, 0);
-      R.mean8.assign(8 * nc, 0);
+      R.mean8.assign((size_t)ori.np * nc, 0);
       if (P.want_diag) {
         R.bin_margin.assign(nc, std::numeric_limits<T>::infinity());
         R.var_cond.assign(nc, std::numeric_limits<T>::infinity());
@@ -363,7 +406,8 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
       for (int y = 0; y < hc; ++y)
         for (int x = 0; x < wc; ++x) {
           const size_t o = (size_t)y * wc + x;
-          T wsum = 0, wsum2 = 0, I[2] = {0, 0}, V[2] = {0, 0};
+          const int dim = ori.d;
+          T wsum = 0, wsum2 = 0, I[3] = {0, 0, 0}, V[3] = {0, 0, 0};
           for (int a = 0; a < sws; ++a)
             for (int b = 0; b < sws; ++b) {
               const T w = wfull[(size_t)(a * sws + b) * nc + o];
@@ -371,8 +415,8 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
               const int ny = y + a + Psh + Ssh, nx = x + b + Psh + Ssh;
               wsum += w;
               wsum2 += w * w;
-              for (int d = 0; d < 2; ++d) {
-                const T inten = ori.at(d * 6, ny, nx);
+              for (int d = 0; d < dim; ++d) {
+                const T inten = ori.at(ori.plane(d, d), ny, nx);
                 const T insq = inten * inten;
                 I[d] += w * inten;
                 V[d] += w * insq;
@@ -380,8 +424,8 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
               if (P.want_diag) R.bin_margin[o] = std::min(R.bin_margin[o], fmargin[(size_t)(a * sws + b) * nc + o]);
             }
           const T enl = wsum * wsum / wsum2;
-          T var[2], inl[2];
-          for (int d = 0; d < 2; ++d) {
+          T var[3], inl[3];
+          for (int d = 0; d < dim; ++d) {
             I[d] /= wsum;
             V[d] /= wsum;
             var[d] = V[d] - I[d] * I[d];
@@ -390,7 +434,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
           }
           // compute_alphas.cl:30-42 (nlooks = 1)
           T alpha = 0;
-          for (int d = 0; d < 2; ++d)
+          for (int d = 0; d < dim; ++d)
             alpha = cl_max<T>(alpha, cl_max<T>(T(0), (var[d] - inl[d] * inl[d] / T(1)) / var[d]));
           // compute_enls_nobias.cl:19-23
           const T oma = T(1) - alpha;
@@ -398,8 +442,8 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
           R.enl_nobias[o] = enb;
           R.alpha[o] = alpha;
           R.wsum[o] = wsum;
-          // weighted means of all 8 planes (weighted_means.cl:47-80), kept per combo
-          for (int pl = 0; pl < 8; ++pl) {
+          // weighted means of every plane (weighted_means.cl:47-80), kept per combo
+          for (int pl = 0; pl < ori.np; ++pl) {
             T cnew = 0, ws = 0;
             for (int a = 0; a < sws; ++a)
               for (int b = 0; b < sws; ++b) {
@@ -435,7 +479,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
       if (combos[i].p == k.first && combos[i].s == k.second) return i;
     return -1;
   };
-  out.cov8.assign(8 * nc, 0);
+  out.cov8.assign((size_t)ori.np * nc, 0);
   out.sel.assign(nc, 0);
   if (P.want_diag) {
     out.bin_margin.assign(nc, 0);
@@ -486,7 +530,7 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
     }
     out.sel[o] = sel;
     const int y = (int)(o / wc), x = (int)(o % wc);
-    for (int pl = 0; pl < 8; ++pl) {
+    for (int pl = 0; pl < ori.np; ++pl) {
       const T cnew = res[sel].mean8[(size_t)pl * nc + o];
       const T ws = res[sel].wsum[o];
       const T center = ori.at(pl, y + wsh + Ssh + Psh, x + wsh + Ssh + Psh);
@@ -536,8 +580,8 @@ std::vector<TileRect> tile_list(int H, int W, int th, int tw, int ov) {
 // get_sub_image with clamp padding (sub_images.cpp:23-45)
 template <typename T>
 Cov<T> cov_tile(const Cov<T>& img, int h0, int w0, int th, int tw) {
-  Cov<T> c(th, tw);
-  for (int pl = 0; pl < 8; ++pl)
+  Cov<T> c(th, tw, img.d);
+  for (int pl = 0; pl < img.np; ++pl)
     for (int y = 0; y < th; ++y)
       for (int x = 0; x < tw; ++x) {
         const int yy = std::min(img.h - 1, std::max(0, y + h0));
@@ -576,7 +620,7 @@ int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w
     const Cov<T> tile = cov_tile<T>(img, tiles[t].h0, tiles[t].w0, tile_h, tile_w);
     outs[t] = filter_tile<T>(tile, P);
   }
-  outc = Cov<T>(H, W);
+  outc = Cov<T>(H, W, img.d);
   if (sel) sel->assign((size_t)H * W, 0);
   if (bmar) bmar->assign((size_t)H * W, 0);
   if (emar) emar->assign((size_t)H * W, 0);
@@ -593,7 +637,7 @@ int nlsar_image(const Cov<T>& img, const FilterParams& P, int tile_h, int tile_w
         const int yy = std::min(H - 1, std::max(0, tiles[t].h0 + ov + y));
         const int xx = std::min(W - 1, std::max(0, tiles[t].w0 + ov + x));
         const size_t oi = (size_t)y * o.wc + x;
-        for (int pl = 0; pl < 8; ++pl) outc.at(pl, yy, xx) = o.cov8[(size_t)pl * o.hc * o.wc + oi];
+        for (int pl = 0; pl < img.np; ++pl) outc.at(pl, yy, xx) = o.cov8[(size_t)pl * o.hc * o.wc + oi];
         if (sel) (*sel)[(size_t)yy * W + xx] = o.sel[oi];
         if (bmar && !o.bin_margin.empty()) (*bmar)[(size_t)yy * W + xx] = o.bin_margin[oi];
         if (emar && !o.enl_margin.empty()) (*emar)[(size_t)yy * W + xx] = o.enl_margin[oi];
@@ -660,9 +704,9 @@ int run_insar(const float* a1, const float* a2, const float* ph, float* ref, flo
 }
 
 template <typename T>
-int run_covmat(const float* cin, float* cout, int H, int W, const FilterParams& P, int tile_h, int tile_w,
+int run_covmat(const float* cin, float* cout, int H, int W, int dim, const FilterParams& P, int tile_h, int tile_w,
                int nthreads) {
-  Cov<T> img(H, W);
+  Cov<T> img(H, W, dim);
   for (size_t i = 0; i < img.v.size(); ++i) img.v[i] = cin[i];
   Cov<T> outc;
   int rc = nlsar_image<T>(img, P, tile_h, tile_w, nthreads, outc, nullptr, nullptr, nullptr, nullptr);
@@ -695,16 +739,16 @@ extern "C" int oracle_nlsar_insar(const float* a1, const float* a2, const float*
                           enl_margin, var_cond, kappa, bin_margin_all);
 }
 
-extern "C" int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int sws, const int* patches,
+extern "C" int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int dim, int sws, const int* patches,
                                    int np, const int* scales, int ns, const oracle_lut* luts, int nluts,
                                    float h, float c, int select_mode, int use_double, int tile_h, int tile_w,
                                    int nthreads) {
   FilterParams P;
   int rc = build_params(P, sws, patches, np, scales, ns, luts, nluts, h, c, select_mode, 0);
   if (rc) return rc;
-  if (H < 1 || W < 1) return -1;
-  if (use_double) return run_covmat<double>(cin, cout, H, W, P, tile_h, tile_w, nthreads);
-  return run_covmat<float>(cin, cout, H, W, P, tile_h, tile_w, nthreads);
+  if (H < 1 || W < 1 || dim < 2 || dim > 3) return -1;
+  if (use_double) return run_covmat<double>(cin, cout, H, W, dim, P, tile_h, tile_w, nthreads);
+  return run_covmat<float>(cin, cout, H, W, dim, P, tile_h, tile_w, nthreads);
 }
 
 extern "C" int oracle_overlap(int sws, const int* patches, int np, const int* scales, int ns) {
@@ -722,12 +766,16 @@ extern "C" float oracle_pixel_similarity_2x2(float a00, float a01r, float a01i, 
   return glr_2x2<float>(a00, a01r, a01i, a11, b00, b01r, b01i, b11);
 }
 
+// a, b: the 9 unique reals {a00, a11, a22, Re a01, Im a01, Re a02, Im a02, Re a12, Im a12}
+extern "C" float oracle_pixel_similarity_3x3(const float* a, const float* b) { return glr_3x3<float>(a, b); }
+
 extern "C" void oracle_gen_gauss(int s, float* out) {
   const std::vector<float> g = gen_gauss<float>(s);
   std::copy(g.begin(), g.end(), out);
 }
 
-extern "C" float oracle_rescale_gamma(void) { return rescale_gamma<float>(); }
+extern "C" float oracle_rescale_gamma(void) { return rescale_gamma<float>(2); }
+extern "C" float oracle_rescale_gamma_dim(int dim) { return rescale_gamma<float>(dim); }
 
 extern "C" void oracle_covmat_create(const float* a1, const float* a2, const float* ph, int H, int W, float* cov8) {
   const Cov<float> c = covmat_create<float>(a1, a2, ph, H, W);

@@ -23,13 +23,15 @@ int oracle_nlsar_insar(const float* a1, const float* a2, const float* ph, float*
                        const oracle_lut* luts, int nluts, float h, float c, int select_mode, int use_double,
                        int tile_h, int tile_w, int nthreads, int* sel, double* bin_margin, double* enl_margin,
                        double* var_cond, double* kappa, double* bin_margin_all);
-int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int sws, const int* patches, int np,
+int oracle_nlsar_covmat(const float* cin, float* cout, int H, int W, int dim, int sws, const int* patches, int np,
                         const int* scales, int ns, const oracle_lut* luts, int nluts, float h, float c,
                         int select_mode, int use_double, int tile_h, int tile_w, int nthreads);
+float oracle_pixel_similarity_3x3(const float* a, const float* b);
+float oracle_rescale_gamma_dim(int dim);
 int oracle_overlap(int sws, const int* patches, int np, const int* scales, int ns);
 
 // training: dissimilarities and LUTs
-long oracle_training_dissims(const float* cov8, int H, int W, int patch, int scale, float* out, long cap);
+long oracle_training_dissims(const float* cov, int H, int W, int dim, int patch, int scale, float* out, long cap);
 int oracle_stats_from_dissims(const float* dissims, long n, unsigned lut_size, float* dmin, float* dmax,
                               float* quantilles, float* chi2cdf_inv);
 double oracle_chi2_inv(double y, double nu);

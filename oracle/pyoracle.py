@@ -48,6 +48,8 @@ def lib():
         _LIB.oracle_pixel_similarity_2x2.restype = ctypes.c_float
         _LIB.oracle_pixel_similarity_2x2.argtypes = [ctypes.c_float] * 8
         _LIB.oracle_rescale_gamma.restype = ctypes.c_float
+        _LIB.oracle_rescale_gamma_dim.restype = ctypes.c_float
+        _LIB.oracle_pixel_similarity_3x3.restype = ctypes.c_float
         _LIB.oracle_lut_weight.restype = ctypes.c_float
         _LIB.oracle_alpha.restype = ctypes.c_float
         _LIB.oracle_enl_nobias.restype = ctypes.c_float
@@ -66,6 +68,7 @@ def ref_pieces():
         _REF.ref_pixel_similarity_2x2.restype = ctypes.c_float
         _REF.ref_pixel_similarity_2x2.argtypes = [ctypes.c_float] * 8
         _REF.ref_det_covmat_3x3.restype = ctypes.c_float
+        _REF.ref_pixel_similarity_3x3.restype = ctypes.c_float
     return _REF
 
 
@@ -141,14 +144,17 @@ def nlsar_insar(a1, a2, phi, sws, patches, scales, stats, h=15.0, c=49.0, select
 
 def nlsar_covmat(cov8, sws, patches, scales, stats, h=15.0, c=49.0, select_mode=0, use_double=False, tile=None,
                  nthreads=0):
+    """cov8: [2*d*d][H][W] covariance planes (d = 2 or 3; even planes real,
+    odd planes imaginary)."""
     cov8 = _f32(cov8)
-    _, H, W = cov8.shape
+    npl, H, W = cov8.shape
+    dim = {8: 2, 18: 3}[npl]
     out = np.zeros_like(cov8)
     p = np.array(patches, np.int32)
     s = np.array(scales, np.int32)
     luts, keep = _luts(stats)
     th, tw = tile if tile else default_tile(H, W, sws, patches, scales)
-    rc = lib().oracle_nlsar_covmat(_fp(cov8), _fp(out), H, W, sws, _ip(p), len(p), _ip(s), len(s), luts,
+    rc = lib().oracle_nlsar_covmat(_fp(cov8), _fp(out), H, W, dim, sws, _ip(p), len(p), _ip(s), len(s), luts,
                                    len(stats), ctypes.c_float(h), ctypes.c_float(c), select_mode, int(use_double),
                                    th, tw, nthreads)
     if rc != 0:
@@ -210,12 +216,25 @@ def training_insar(a1, a2, phi, patches, scales):
 
 
 def training_dissims(cov8, patch, scale):
+    """cov8: [2*d*d][H][W] covariance planes, d = 2 or 3."""
     cov8 = _f32(cov8)
-    _, H, W = cov8.shape
-    n = lib().oracle_training_dissims(_fp(cov8), H, W, patch, scale, None, ctypes.c_long(0))
+    npl, H, W = cov8.shape
+    dim = {8: 2, 18: 3}[npl]
+    n = lib().oracle_training_dissims(_fp(cov8), H, W, dim, patch, scale, None, ctypes.c_long(0))
     out = np.zeros(n, np.float32)
-    lib().oracle_training_dissims(_fp(cov8), H, W, patch, scale, _fp(out), ctypes.c_long(n))
+    lib().oracle_training_dissims(_fp(cov8), H, W, dim, patch, scale, _fp(out), ctypes.c_long(n))
     return out
+
+
+def training_covmat(cov, patches, scales):
+    """nlsar_training on a covariance image [2*d*d][H][W]: stats per (patch, scale)."""
+    return {(int(p), int(s)): stats_from_dissims(training_dissims(cov, p, s)) for p in patches for s in scales}
+
+
+def pixel_similarity_3x3(a, b):
+    a = _f32(np.asarray(a).ravel())
+    b = _f32(np.asarray(b).ravel())
+    return lib().oracle_pixel_similarity_3x3(_fp(a), _fp(b))
 
 
 def stats_from_dissims(d, lut_size=256):

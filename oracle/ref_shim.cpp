@@ -19,6 +19,12 @@ extern "C" float ref_pixel_similarity_2x2(float a00, float a01r, float a01i, flo
   return pixel_similarity_2x2(a00, a01r, a01i, a11, b00, b01r, b01i, b11, 1);
 }
 
+// a, b: {a00, a11, a22, Re a01, Im a01, Re a02, Im a02, Re a12, Im a12}
+extern "C" float ref_pixel_similarity_3x3(const float* a, const float* b) {
+  return pixel_similarity_3x3(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], b[0], b[1], b[2], b[3], b[4], b[5],
+                              b[6], b[7], b[8], 1);
+}
+
 extern "C" float ref_det_covmat_3x3(const float* a) {
   return det_covmat_3x3(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]);
 }

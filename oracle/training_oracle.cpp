@@ -92,9 +92,9 @@ double chi2_inv(double y, double nu) {
   return x;
 }
 
-// 8-plane covariance image [8][h][w]
+// covariance image [2*d*d][h][w], d = 2 or 3
 struct Cov {
-  int h, w;
+  int h, w, d;
   std::vector<float> v;
   float& at(int p, int y, int x) { return v[((size_t)p * h + y) * w + x]; }
   float at(int p, int y, int x) const { return v[((size_t)p * h + y) * w + x]; }
@@ -114,13 +114,38 @@ inline float glr(float a00, float a01r, float a01i, float a11, float b00, float 
   return sim;
 }
 
-Cov rescaled_avg(const float* cov8, int H, int W, int s) {
-  // get_dissims.cpp:84-100: rescale in place, then spatial average with
+inline float det3(float a00, float a11, float a22, float a01r, float a01i, float a02r, float a02i, float a12r,
+                  float a12i) {
+  // sim_measures.h:66-97
+  return a00 * a11 * a22 - a00 * (a12r * a12r + a12i * a12i) - a11 * (a02r * a02r + a02i * a02i) -
+         a22 * (a01r * a01r + a01i * a01i) +
+         2 * (a01r * a12r * a02r - a01i * a12i * a02r + a01r * a12i * a02i + a01i * a12r * a02i);
+}
+
+// a, b: {a00, a11, a22, Re a01, Im a01, Re a02, Im a02, Re a12, Im a12} (sim_measures.h:100-160)
+inline float glr3(const float* a, const float* b) {
+  const float nom1 = det3(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]);
+  const float nom2 = det3(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8]);
+  const float det = det3(a[0] + b[0], a[1] + b[1], a[2] + b[2], a[3] + b[3], a[4] + b[4], a[5] + b[5], a[6] + b[6],
+                         a[7] + b[7], a[8] + b[8]);
+  float sim = -1 * (2 * 3 * std::log(2.0f) + std::log(nom1) + std::log(nom2) - 2 * std::log(det));
+  if (std::isnan(sim)) sim = 0;
+  return sim;
+}
+
+Cov rescaled_avg(const float* cov, int H, int W, int dim, int s) {
+  // get_dissims.cpp:84-100: rescale in place (covmat_rescale.cl: every
+  // off-diagonal element times (1/dim)^0.33333), then spatial average with
   // scale_size_max = scale_size
-  Cov r{H, W, std::vector<float>(cov8, cov8 + (size_t)8 * H * W)};
-  const float gamma = std::pow(std::min(1.0f / 2, 1.0f), 0.33333f);
-  for (int pl = 2; pl <= 5; ++pl)
-    for (size_t i = 0; i < (size_t)H * W; ++i) r.v[(size_t)pl * H * W + i] *= gamma;
+  const int npl = 2 * dim * dim;
+  Cov r{H, W, dim, std::vector<float>(cov, cov + (size_t)npl * H * W)};
+  const float gamma = std::pow(std::min(1.0f / dim, 1.0f), 0.33333f);
+  for (int row = 0; row < dim; ++row)
+    for (int col = 0; col < dim; ++col) {
+      if (row == col) continue;
+      for (int pl = 2 * (row * dim + col); pl <= 2 * (row * dim + col) + 1; ++pl)
+        for (size_t i = 0; i < (size_t)H * W; ++i) r.v[(size_t)pl * H * W + i] *= gamma;
+    }
   const int ssh = (s - 1) / 2;
   std::vector<float> g;
   for (int x = -ssh; x <= ssh; ++x)
@@ -129,8 +154,8 @@ Cov rescaled_avg(const float* cov8, int H, int W, int s) {
   float K = 0;
   for (float e : g) K += e;
   for (float& e : g) e = e / K;
-  Cov o{H - s + 1, W - s + 1, std::vector<float>((size_t)8 * (H - s + 1) * (W - s + 1))};
-  for (int pl = 0; pl < 8; ++pl)
+  Cov o{H - s + 1, W - s + 1, dim, std::vector<float>((size_t)npl * (H - s + 1) * (W - s + 1))};
+  for (int pl = 0; pl < npl; ++pl)
     for (int y = 0; y < o.h; ++y)
       for (int x = 0; x < o.w; ++x) {
         float sum = 0;
@@ -141,22 +166,24 @@ Cov rescaled_avg(const float* cov8, int H, int W, int s) {
   return o;
 }
 
-std::vector<float> dissims_of(const float* cov8, int H, int W, int p, int s) {
-  const Cov a = rescaled_avg(cov8, H, W, s);
-  // patches.cpp:32-41: tile_iterator(h, w, p, p, 0, 0), clamp padding
-  struct Patch { std::vector<float> e00, e01r, e01i, e11; };
-  std::vector<Patch> patches;
+std::vector<float> dissims_of(const float* cov, int H, int W, int dim, int p, int s) {
+  const Cov a = rescaled_avg(cov, H, W, dim, s);
+  // patches.cpp:32-41: tile_iterator(h, w, p, p, 0, 0), clamp padding.  Each
+  // patch pixel keeps the planes its similarity reads (patches.cpp:70-136):
+  // 2x2 {0, 2, 3, 6}, 3x3 {0, 8, 16, 2, 3, 4, 5, 10, 11}
+  static const int pl2[4] = {0, 2, 3, 6};
+  static const int pl3[9] = {0, 8, 16, 2, 3, 4, 5, 10, 11};
+  const int nv = dim == 2 ? 4 : 9;
+  const int* pl = dim == 2 ? pl2 : pl3;
+  std::vector<std::vector<float>> patches;
   for (int h0 = 0; h0 < a.h; h0 += p)
     for (int w0 = 0; w0 < a.w; w0 += p) {
-      Patch P;
+      std::vector<float> P;
       for (int y = 0; y < p; ++y)
         for (int x = 0; x < p; ++x) {
           const int yy = std::min(a.h - 1, std::max(0, h0 + y));
           const int xx = std::min(a.w - 1, std::max(0, w0 + x));
-          P.e00.push_back(a.at(0, yy, xx));
-          P.e01r.push_back(a.at(2, yy, xx));
-          P.e01i.push_back(a.at(3, yy, xx));
-          P.e11.push_back(a.at(6, yy, xx));
+          for (int k = 0; k < nv; ++k) P.push_back(a.at(pl[k], yy, xx));
         }
       patches.push_back(std::move(P));
     }
@@ -165,13 +192,13 @@ std::vector<float> dissims_of(const float* cov8, int H, int W, int p, int s) {
   const size_t n = patches.size();
   d.reserve(n * (n - 1) / 2);
   for (size_t hi = n; hi-- > 1;) {
-    const Patch& head = patches[hi];
+    const std::vector<float>& head = patches[hi];
     for (size_t j = 0; j < hi; ++j) {
-      const Patch& o = patches[j];
+      const std::vector<float>& o = patches[j];
       float sum = 0.0f;
-      for (size_t i = 0; i < head.e00.size(); ++i)
-        sum += glr(head.e00[i], head.e01r[i], head.e01i[i], head.e11[i], o.e00[i], o.e01r[i], o.e01i[i],
-                   o.e11[i]);
+      for (size_t i = 0; i < head.size(); i += nv)
+        sum += dim == 2 ? glr(head[i], head[i + 1], head[i + 2], head[i + 3], o[i], o[i + 1], o[i + 2], o[i + 3])
+                        : glr3(&head[i], &o[i]);
       d.push_back(sum);
     }
   }
@@ -204,9 +231,10 @@ void stats_of(std::vector<float> d, unsigned L, float* dmin, float* dmax, float*
 
 extern "C" double oracle_chi2_inv(double y, double nu) { return chi2_inv(y, nu); }
 
-extern "C" long oracle_training_dissims(const float* cov8, int H, int W, int patch, int scale, float* out,
+extern "C" long oracle_training_dissims(const float* cov, int H, int W, int dim, int patch, int scale, float* out,
                                         long cap) {
-  const std::vector<float> d = dissims_of(cov8, H, W, patch, scale);
+  if (dim < 2 || dim > 3) return -1;
+  const std::vector<float> d = dissims_of(cov, H, W, dim, patch, scale);
   if (out) std::copy(d.begin(), d.begin() + std::min<long>(cap, (long)d.size()), out);
   return (long)d.size();
 }
@@ -240,7 +268,7 @@ extern "C" int oracle_nlsar_training_insar(const float* a1, const float* a2, con
   int k = 0;
   for (int pi = 0; pi < np; ++pi)
     for (int si = 0; si < ns; ++si, ++k) {
-      const std::vector<float> d = dissims_of(cov.data(), H, W, patches[pi], scales[si]);
+      const std::vector<float> d = dissims_of(cov.data(), H, W, 2, patches[pi], scales[si]);
       out_patch[k] = patches[pi];
       out_scale[k] = scales[si];
       stats_of(d, 256, out_dmin + k, out_dmax + k, out_quant + (size_t)k * 256, out_chi2 + (size_t)k * 256);
