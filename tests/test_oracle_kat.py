@@ -219,3 +219,81 @@ def test_training_pair_counts(oracle):
         hs = 64 - s + 1
         n = (-(-hs // p)) ** 2
         assert oracle.training_dissims(cov, p, s).size == n * (n - 1) // 2
+
+
+def _herm3(rng):
+    """A random Hermitian positive-definite 3x3 matrix as its 9 unique reals
+    {a00, a11, a22, Re a01, Im a01, Re a02, Im a02, Re a12, Im a12}."""
+    z = rng.normal(size=(3, 4)) + 1j * rng.normal(size=(3, 4))
+    m = z @ z.conj().T / 4
+    return np.float32([m[0, 0].real, m[1, 1].real, m[2, 2].real, m[0, 1].real, m[0, 1].imag, m[0, 2].real,
+                       m[0, 2].imag, m[1, 2].real, m[1, 2].imag])
+
+
+def test_similarity_3x3_matches_reference_translation_unit(oracle):
+    ref = oracle.ref_pieces()
+    if ref is None:
+        pytest.skip("reference source tree absent: pieces not built")
+    rng = np.random.default_rng(5)
+    fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))  # noqa: E731
+    for _ in range(2000):
+        a, b = _herm3(rng), _herm3(rng)
+        assert oracle.pixel_similarity_3x3(a, b) == ref.ref_pixel_similarity_3x3(fp(a), fp(b))
+    # identical pixels: 0; a singular pixel next to a regular one: +inf
+    a = _herm3(rng)
+    assert oracle.pixel_similarity_3x3(a, a) == pytest.approx(0.0, abs=1e-4)
+    s = np.float32([1, 1, 1, 1, 0, 1, 0, 1, 0])  # rank one: all-ones matrix
+    assert np.isinf(oracle.pixel_similarity_3x3(s, a))
+
+
+def test_rescale_gamma_3x3(oracle):
+    # covmat_rescale.cl:25-26: (1/dim)^0.33333
+    assert oracle.lib().oracle_rescale_gamma_dim(3) == pytest.approx((1 / 3) ** 0.33333, rel=1e-6)
+    assert oracle.lib().oracle_rescale_gamma_dim(2) == oracle.lib().oracle_rescale_gamma()
+
+
+def _cov18(m9, H, W):
+    """A constant 18-plane covariance image from the 9 unique reals (the
+    lower triangle the conjugate of the upper)."""
+    a00, a11, a22, r01, i01, r02, i02, r12, i12 = [float(x) for x in m9]
+    M = np.array([[a00, r01 + 1j * i01, r02 + 1j * i02],
+                  [r01 - 1j * i01, a11, r12 + 1j * i12],
+                  [r02 - 1j * i02, r12 - 1j * i12, a22]])
+    cov = np.zeros((18, H, W), np.float32)
+    for r in range(3):
+        for c in range(3):
+            cov[2 * (r * 3 + c)] = M[r, c].real
+            cov[2 * (r * 3 + c) + 1] = M[r, c].imag
+    return cov
+
+
+def test_filter_of_constant_3x3_scene_is_constant(oracle):
+    # compute_nl_statistics_test.cpp / weighted_means_test.cpp for 3x3: with
+    # power-of-two entries every weighted mean is exact, the variance exactly
+    # 0 and alpha 0, so a constant scene comes back unchanged
+    rng = np.random.default_rng(6)
+    m = np.float32([4, 2, 1, 0.5, 0.25, 0.25, -0.5, 0.125, 0.125])
+    # training on a speckled 3-channel area gives LUTs with a sane spread
+    z = (rng.normal(size=(3, 40, 40)) + 1j * rng.normal(size=(3, 40, 40))) / np.sqrt(2)
+    train = np.zeros((18, 40, 40), np.float32)
+    for r in range(3):
+        for c in range(3):
+            e = z[r] * z[c].conj()
+            train[2 * (r * 3 + c)] = e.real
+            train[2 * (r * 3 + c) + 1] = e.imag
+    stats = oracle.training_covmat(train, [3, 5], [1, 3])
+    cov = _cov18(m, 36, 40)
+    for dbl in (False, True):
+        out = oracle.nlsar_covmat(cov, 11, [3, 5], [1, 3], stats, select_mode=1, use_double=dbl)
+        np.testing.assert_array_equal(out, cov)
+
+
+def test_training_3x3_pair_counts(oracle):
+    rng = np.random.default_rng(7)
+    cov = _cov18(_herm3(rng), 30, 30) * rng.uniform(0.5, 1.5, (1, 30, 30)).astype(np.float32)
+    for p, s in [(3, 1), (5, 3)]:
+        n = -(-(30 - s + 1) // p)
+        n = n * n
+        d = oracle.training_dissims(cov, p, s)
+        assert d.size == n * (n - 1) // 2
+        assert np.isfinite(d).all()
