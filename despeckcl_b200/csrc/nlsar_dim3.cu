@@ -1,0 +1,641 @@
+// NL-SAR on 3x3 (PolSAR) covariance images: despeckcl::nlsar with dim = 3
+// (src/compute/nlsar/nlsar.cpp:171-194 in the reference, the same per-tile
+// pipeline as the 2x2 case, nlsar_filter_sub_image.cpp:146-390) and
+// despeckcl::nlsar_training on such images (training/get_dissims.cpp,
+// training/patches.cpp:43-136).
+//
+// Differences from the 2x2 path, all following the reference (paths relative
+// to src/compute/nlsar/):
+//  * the covariance has 18 planes, plane 2(r*3+c) the real and 2(r*3+c)+1
+//    the imaginary part of element (r, c);
+//  * the rescale factor is (1/3)^0.33333 (cl_kernels/covmat_rescale.cl:25-26);
+//  * the pixel similarity is the 3x3 GLR of
+//    cl_kernels/compute_pixel_similarities_3x3.cl.in with
+//    sim_measures.h:66-160 (Leibniz determinant of a Hermitian matrix from its
+//    diagonal and upper triangle);
+//  * statistics and alpha run over the three diagonal intensities
+//    (cl_kernels/compute_nl_statistics.cl, compute_alphas.cl);
+//  * the weighted means cover all 18 planes (cl_kernels/weighted_means.cl).
+//
+// Layout: the padded frame of the 2x2 engine (virtual plane, clamp padding),
+// stored planar: c18 [18][Hp][pitch] (un-rescaled covariance) and, per scale,
+// s9 [9][Hp][pitch] (the nine similarity reals of the rescaled, Gaussian-
+// averaged covariance: a00, a11, a22, Re/Im a01, Re/Im a02, Re/Im a12) plus
+// ld [Hp][pitch] (their ln det).  The fused kernel keeps one 32 x 8 output tile
+// per CTA (one pixel per thread): per offset batch it computes the
+// similarities of the tile plus patch halo from the staged s9 region, the
+// horizontal sums of every patch size of the pass, then per pixel the
+// vertical sums, the composite LUT weight and 23 accumulators per patch size
+// (sum w, w^2, w I_d^2 for d = 0..2, and w times each of the 18 planes, read
+// through the L1 cache); the epilogue derives ENL, alpha and ENL', selects and
+// blends with the centre pixel.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <vector>
+
+#include "../../include/despeckcl_b200.h"
+#include "dcl_internal.h"
+#include "nlsar_common.cuh"
+#include "nlsar_plan.h"
+#include "stats_internal.h"
+
+namespace dcl {
+
+std::vector<float> gauss_weights(int s);
+
+namespace {
+
+constexpr int kT3W = 32;        // output columns per tile (one lane per column)
+constexpr int kT3Warps = 8;     // warps per CTA, one output row each
+constexpr int kT3H = kT3Warps;  // output rows per tile
+constexpr int kT3Threads = 32 * kT3Warps;
+constexpr int kNA3 = 23;        // accumulators per patch size
+
+// planes of the nine similarity reals within the 18 covariance planes
+__host__ __device__ constexpr int sim_plane(int k) {
+  return k == 0 ? 0 : k == 1 ? 8 : k == 2 ? 16 : k == 3 ? 2 : k == 4 ? 3 : k == 5 ? 4 : k == 6 ? 5 : k == 7 ? 10 : 11;
+}
+// planes of the diagonal intensities
+__host__ __device__ constexpr int diag_plane(int d) { return 8 * d; }
+
+__device__ __forceinline__ int clamp3(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// sim_measures.h:78-97 with a = {a00, a11, a22, Re a01, Im a01, Re a02, Im a02, Re a12, Im a12}
+__host__ __device__ __forceinline__ float det3f(const float* a) {
+  return a[0] * a[1] * a[2] - a[0] * (a[7] * a[7] + a[8] * a[8]) - a[1] * (a[5] * a[5] + a[6] * a[6]) -
+         a[2] * (a[3] * a[3] + a[4] * a[4]) +
+         2.0f * (a[3] * a[7] * a[5] - a[4] * a[8] * a[5] + a[3] * a[8] * a[6] + a[4] * a[7] * a[6]);
+}
+
+struct Scene3 {
+  const float* c18;             // [18][Hp][pitch]
+  const float* s9[kMaxScales];  // [9][Hp][pitch] per scale slot
+  const float* ld[kMaxScales];  // [Hp][pitch] per scale slot
+  float* out;                   // [18][H][W]
+  int H, W, vH, vW, pitch, tiles_x;
+  size_t plane;                 // Hp * pitch
+};
+
+struct Smem3 {
+  int rs_w, rs_h, sim_w, sim_h;
+  int off_ld, off_sim, off_h, off_w, total;  // in 4-byte words; s9 planes start at 0
+};
+
+__host__ __device__ inline Smem3 smem3_layout(int wsh, int phm, int K) {
+  Smem3 L;
+  L.rs_w = kT3W + 2 * (phm + wsh);
+  L.rs_h = kT3H + 2 * (phm + wsh);
+  L.sim_w = kT3W + 2 * phm;
+  L.sim_h = kT3H + 2 * phm;
+  int o = 9 * L.rs_w * L.rs_h;
+  L.off_ld = o;
+  o += L.rs_w * L.rs_h;
+  L.off_sim = o;
+  o += K * L.sim_w * L.sim_h;
+  L.off_h = o;
+  o += K * kPatchPerPass * L.sim_h * kT3W;
+  L.off_w = o;
+  o += kPatchPerPass * kMaxLut;
+  L.total = o;
+  return L;
+}
+
+// 18 planes of the clamp-padded frame (sub_images.cpp:37-38 clamping)
+__global__ void prep3_cov_kernel(const float* __restrict__ cin, int H, int W, float* __restrict__ c18, int Hp, int Wp,
+                                 int pitch, size_t plane, int G) {
+  const int px = blockIdx.x * blockDim.x + threadIdx.x;
+  const int py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= Hp) return;
+  const int y = clamp3(py - G, 0, H - 1), x = clamp3(px - G, 0, W - 1);
+  const size_t n = (size_t)H * W, i = (size_t)y * W + x, o = (size_t)py * pitch + px;
+#pragma unroll
+  for (int p = 0; p < 18; ++p) c18[p * plane + o] = cin[p * n + i];
+}
+
+// rescaled (off-diagonals x gamma, covmat_rescale.cl:31-39) and Gaussian
+// averaged (covmat_spatial_avg.cl:50-57) similarity planes of one scale, and
+// their ln det
+__global__ void prep3_scale_kernel(const float* __restrict__ c18, int Hp, int Wp, int pitch, size_t plane, int s,
+                                   GaussArg ga, float gamma, float* __restrict__ s9, float* __restrict__ ld) {
+  const int px = blockIdx.x * blockDim.x + threadIdx.x;
+  const int py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= Hp) return;
+  const int ssh = (s - 1) / 2;
+  float a[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) a[k] = 0.0f;
+  for (int kx = 0; kx < s; ++kx) {
+    const int yy = clamp3(py - ssh + kx, 0, Hp - 1);
+    for (int ky = 0; ky < s; ++ky) {
+      const int xx = clamp3(px - ssh + ky, 0, Wp - 1);
+      const size_t q = (size_t)yy * pitch + xx;
+      const float g = ga.g[kx * s + ky];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const float v = c18[sim_plane(k) * plane + q];
+        a[k] = fmaf(g, k >= 3 ? v * gamma : v, a[k]);
+      }
+    }
+  }
+  const size_t o = (size_t)py * pitch + px;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) s9[k * plane + o] = a[k];
+  ld[o] = logf(det3f(a));
+}
+
+__device__ __forceinline__ void offset3_of(int t, int sws, int wsh, int& dy, int& dx, bool& lower) {
+  // pairs: upper-half slot u of the reference's half-window volume
+  // (compute_pixel_similarities_3x3: quadrants as the 2x2 wrapper), then its
+  // mirror -u (copy_symm_weights.cl:56-76)
+  const int u = t >> 1;
+  const int hh = u / sws, ww = u - hh * sws;
+  dy = hh - wsh;
+  dx = ww - wsh;
+  lower = (t & 1) != 0;
+  if (lower) {
+    dy = -dy;
+    dx = -dx;
+  }
+}
+
+__global__ void __launch_bounds__(kT3Threads, 1) nlsar3_kernel(const FilterParams P, const Scene3 S) {
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  const int tid = threadIdx.x, lane = tid & 31, y = tid >> 5;
+  const int wsh = P.wsh, phm = P.phm, sws = P.sws, G = P.G;
+  const Smem3 L = smem3_layout(wsh, phm, P.K);
+  const int rsn = L.rs_w * L.rs_h;
+  float* sS = smem;
+  float* sLd = smem + L.off_ld;
+  float* sSim = smem + L.off_sim;
+  float* sH = smem + L.off_h;
+  float* sW = smem + L.off_w;
+  const int ty = blockIdx.x / S.tiles_x, tx = blockIdx.x - ty * S.tiles_x;
+  const int vy0 = ty * kT3H, vx0 = tx * kT3W;
+  // frame index of this thread's output pixel
+  const size_t cfi = (size_t)(vy0 + y + G) * S.pitch + (vx0 + lane + G);
+
+  float acc[kPatchPerPass][kNA3];
+  float best_e = -1.0f, best_a = 0.0f, best_s0 = 1.0f, best_m[18];
+  int best_rank = 0x7fffffff, best_combo = -1;
+#pragma unroll
+  for (int p = 0; p < 18; ++p) best_m[p] = 0.0f;
+
+  int loaded_slot = -1;
+  for (int ps = 0; ps < P.npass; ++ps) {
+    const PassParams& pp = P.pass[ps];
+    const int np = pp.np;
+    __syncthreads();
+    if (pp.scale_slot != loaded_slot) {
+      const float* s9 = S.s9[pp.scale_slot];
+      const float* ldp = S.ld[pp.scale_slot];
+      const int by = vy0 - phm - wsh + G, bx = vx0 - phm - wsh + G;
+      for (int i = tid; i < rsn; i += kT3Threads) {
+        const int r = i / L.rs_w, c = i - r * L.rs_w;
+        const size_t g = (size_t)(by + r) * S.pitch + (bx + c);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sS[k * rsn + i] = s9[k * S.plane + g];
+        sLd[i] = ldp[g];
+      }
+      loaded_slot = pp.scale_slot;
+    }
+    for (int i = tid; i < np * kMaxLut; i += kT3Threads) {
+      const int j = i / kMaxLut;
+      sW[i] = P.wtab[pp.combo[j] * kMaxLut + (i - j * kMaxLut)];
+    }
+#pragma unroll
+    for (int j = 0; j < kPatchPerPass; ++j)
+#pragma unroll
+      for (int a = 0; a < kNA3; ++a) acc[j][a] = 0.0f;
+    __syncthreads();
+
+    const int K = P.K;
+    for (int t0 = 0; t0 < P.n_off; t0 += K) {
+      const int kb = min(K, P.n_off - t0);
+      // ---- A: 3x3 similarities of the batch on the tile + patch halo
+      const int nsim = L.sim_w * L.sim_h;
+      for (int i = tid; i < kb * nsim; i += kT3Threads) {
+        const int k = i / nsim;
+        const int rem = i - k * nsim;
+        const int r = rem / L.sim_w, c = rem - r * L.sim_w;
+        int dy, dx;
+        bool lower;
+        offset3_of(t0 + k, sws, wsh, dy, dx, lower);
+        const int ci = (r + wsh) * L.rs_w + (c + wsh);
+        const int ni = ci + dy * L.rs_w + dx;
+        float sum[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) sum[q] = sS[q * rsn + ci] + sS[q * rsn + ni];
+        const float det = det3f(sum);
+        const float la = sLd[ci], lb = sLd[ni];
+        // the mirrored half takes the neighbour as the first argument
+        // (copy_symm_weights.cl:66-74)
+        const float t = lower ? (P.c2d + lb) + la : (P.c2d + la) + lb;
+        float sim = -(t - 2.0f * logf(det));
+        if (sim != sim) sim = 0.0f;
+        sSim[i] = sim;
+      }
+      __syncthreads();
+      // ---- B: horizontal sums for every patch size of the pass (nested rings)
+      const int nh = L.sim_h * kT3W;
+      for (int i = tid; i < kb * nh; i += kT3Threads) {
+        const int k = i / nh;
+        const int rem = i - k * nh;
+        const int r = rem / kT3W, c = rem - r * kT3W;
+        const float* row = sSim + k * nsim + r * L.sim_w + c + phm;
+        float sacc = row[0];
+        int b = 0;
+#pragma unroll
+        for (int j = 0; j < kPatchPerPass; ++j) {
+          if (j < np) {
+            const int ph = pp.ph[j];
+            for (; b < ph;) {
+              ++b;
+              sacc += row[-b] + row[b];
+            }
+            sH[((k * kPatchPerPass + j) * L.sim_h + r) * kT3W + c] = sacc;
+          }
+        }
+      }
+      __syncthreads();
+      // ---- C: vertical sums, weights, accumulation
+      for (int k = 0; k < kb; ++k) {
+        int dy, dx;
+        bool lower;
+        offset3_of(t0 + k, sws, wsh, dy, dx, lower);
+        const size_t nfi = cfi + (ptrdiff_t)dy * S.pitch + dx;
+        float v[18];
+#pragma unroll
+        for (int p = 0; p < 18; ++p) v[p] = __ldg(S.c18 + p * S.plane + nfi);
+        float i2[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) i2[d] = v[diag_plane(d)] * v[diag_plane(d)];
+#pragma unroll
+        for (int j = 0; j < kPatchPerPass; ++j) {
+          if (j < np) {
+            const int ph = pp.ph[j];
+            const ComboParams& cp = P.combo[pp.combo[j]];
+            const float* col = sH + ((k * kPatchPerPass + j) * L.sim_h) * kT3W + lane;
+            float d = 0.0f;
+            for (int a = -ph; a <= ph; ++a) d += col[(y + phm + a) * kT3W];
+            // compute_weights.cl:40-51 through the composite weight table
+            float w;
+            if (d > cp.dmax) {
+              w = 0.0f;
+            } else {
+              float dc = fmaxf(d, cp.dmin);
+              dc = fminf(dc, cp.dmax);
+              const float mapped = __fdiv_rn(dc - cp.dmin, cp.span) * cp.lm1;
+              w = sW[j * kMaxLut + (unsigned)mapped];
+            }
+            float* A = acc[j];
+            A[0] += w;
+            A[1] = fmaf(w, w, A[1]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) A[2 + q] = fmaf(w, i2[q], A[2 + q]);
+#pragma unroll
+            for (int p = 0; p < 18; ++p) A[5 + p] = fmaf(w, v[p], A[5 + p]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---- centre weight 1 (routines.cpp:151-157), statistics, alpha, ENL', selection
+    float c[18];
+#pragma unroll
+    for (int p = 0; p < 18; ++p) c[p] = __ldg(S.c18 + p * S.plane + cfi);
+#pragma unroll
+    for (int j = 0; j < kPatchPerPass; ++j) {
+      if (j < np) {
+        const float* A = acc[j];
+        const float s0 = A[0] + 1.0f, s1 = A[1] + 1.0f;
+        // compute_nl_statistics.cl:92-101 over the three diagonal intensities
+        const float enl = s0 * s0 / s1;
+        float alpha = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float cd = c[diag_plane(d)];
+          const float in = (A[5 + diag_plane(d)] + cd) / s0;
+          const float var = (A[2 + d] + cd * cd) / s0 - in * in;
+          // compute_alphas.cl:30-41 (nlooks = 1)
+          alpha = fmaxf(alpha, fmaxf(0.0f, (var - in * in) / var));
+        }
+        if (P.alpha_zero) alpha = 0.0f;
+        // compute_enls_nobias.cl:19-22
+        const float oma = 1.0f - alpha;
+        const float enb = enl / (oma * oma + (alpha * alpha + 2.0f * alpha * (1.0f - alpha) / s0) * enl);
+        const int combo = pp.combo[j];
+        const int rank = P.combo[combo].rank;
+        const bool take = (P.select_mode == 0) || (enb > best_e) || (enb == best_e && rank < best_rank);
+        const bool take_fb = !take && best_combo < 0 && combo == P.fallback_combo;
+        if (take) {
+          best_e = enb;
+          best_rank = rank;
+        }
+        if (take || take_fb) {
+          best_combo = combo;
+          best_a = alpha;
+          best_s0 = s0;
+#pragma unroll
+          for (int p = 0; p < 18; ++p) best_m[p] = A[5 + p] + c[p];
+        }
+      }
+    }
+  }
+
+  // ---- blend with the centre (weighted_means.cl:79), store the 18 planes
+  const int vy = vy0 + y, vx = vx0 + lane;
+  const int oy = (vy < S.H - 1) ? vy : (vy == S.vH ? S.H - 1 : -1);
+  const int ox = (vx < S.W - 1) ? vx : (vx == S.vW ? S.W - 1 : -1);
+  if (oy < 0 || ox < 0) return;
+  const size_t n = (size_t)S.H * S.W, o = (size_t)oy * S.W + ox;
+  const float oma = 1.0f - best_a;
+#pragma unroll
+  for (int p = 0; p < 18; ++p) {
+    const float cp = __ldg(S.c18 + p * S.plane + cfi);
+    S.out[p * n + o] = oma * best_m[p] / best_s0 + best_a * cp;
+  }
+}
+
+// ---- training ---------------------------------------------------------------
+
+// rescaled and averaged similarity reals on the valid region (H-s+1) x (W-s+1),
+// [pixel][9] (get_dissims.cpp:84-100 with scale_size_max = s)
+__global__ void train3_avg_kernel(const float* __restrict__ cov, int H, int W, int s, GaussArg ga, float gamma,
+                                  float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int Ho = H - s + 1, Wo = W - s + 1;
+  if (x >= Wo || yy >= Ho) return;
+  const size_t n = (size_t)H * W;
+  float a[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) a[k] = 0.0f;
+  for (int kx = 0; kx < s; ++kx)
+    for (int ky = 0; ky < s; ++ky) {
+      const size_t q = (size_t)(yy + kx) * W + x + ky;
+      const float g = ga.g[kx * s + ky];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const float v = cov[sim_plane(k) * n + q];
+        a[k] = fmaf(g, k >= 3 ? v * gamma : v, a[k]);
+      }
+    }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) out[((size_t)yy * Wo + x) * 9 + k] = a[k];
+}
+
+// patches [n][p*p][9], patch k at ((k / nw) * p, (k % nw) * p), clamp padding
+__global__ void train3_gather_kernel(const float* __restrict__ avg, int Ho, int Wo, int p, int nw, int n,
+                                     float* __restrict__ patches) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pp = p * p;
+  if (i >= n * pp) return;
+  const int k = i / pp, r = i - k * pp;
+  const int yy = min(Ho - 1, (k / nw) * p + r / p);
+  const int x = min(Wo - 1, (k % nw) * p + r % p);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) patches[(size_t)i * 9 + q] = avg[((size_t)yy * Wo + x) * 9 + q];
+}
+
+// one thread per unordered pair (hi, j), hi > j: the later patch first
+// (combinations.cpp:26-41, patches.cpp:43-69)
+__global__ void train3_pairs_kernel(const float* __restrict__ patches, int pp, long long npairs, float c2d,
+                                    float* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npairs) return;
+  long long hi = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)t)) * 0.5);
+  while (hi * (hi - 1) / 2 > t) --hi;
+  while ((hi + 1) * hi / 2 <= t) ++hi;
+  const long long j = t - hi * (hi - 1) / 2;
+  const float* A = patches + (size_t)hi * pp * 9;
+  const float* B = patches + (size_t)j * pp * 9;
+  float sum = 0.0f;
+  for (int i = 0; i < pp; ++i) {
+    float a[9], b[9], s[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      a[q] = A[i * 9 + q];
+      b[q] = B[i * 9 + q];
+      s[q] = a[q] + b[q];
+    }
+    // sim_measures.h:100-160, nlooks 1
+    float r = -(c2d + logf(det3f(a)) + logf(det3f(b)) - 2.0f * logf(det3f(s)));
+    if (r != r) r = 0.0f;
+    sum += r;
+  }
+  out[t] = sum;
+}
+
+float rescale_gamma_3x3() {
+  // covmat_rescale.cl:25-26 with nlooks = 1, dimension = 3
+  return std::pow(std::min(1.0f / 3.0f, 1.0f), 0.33333f);
+}
+
+}  // namespace
+
+// NL-SAR of one 3x3 covariance scene on device pointers (planes [18][H][W]).
+int nlsar_covmat3_device(const Plan& pl0, const float* cin, float* cout, int H, int W, cudaStream_t st) {
+  if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  int dev = 0;
+  int rc = ensure_device_ready(dev);
+  if (rc) return rc;
+  Plan pl = pl0;
+  FilterParams& F = pl.P;
+  F.c2d = 2 * 3 * std::log(2.0f);
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || optin <= 0)
+    optin = 227 * 1024;
+  int K = 0;
+  size_t smem = 0;
+  for (int k = 8; k >= 1 && K == 0; --k) {
+    const size_t b = (size_t)smem3_layout(F.wsh, F.phm, k).total * 4;
+    if (b <= (size_t)optin) {
+      K = k;
+      smem = b;
+    }
+  }
+  if (K < 1) return set_error(DCL_ERR_UNSUPPORTED, "search window / patch sizes too large for shared memory");
+  F.K = K;
+  F.tile_h = kT3H;
+
+  Scene3 S;
+  std::memset(&S, 0, sizeof S);
+  S.H = H;
+  S.W = W;
+  S.vH = H - 1 + pl.overlap;
+  S.vW = W - 1 + pl.overlap;
+  const int tiles_y = (S.vH + 1 + kT3H - 1) / kT3H;
+  S.tiles_x = (S.vW + 1 + kT3W - 1) / kT3W;
+  const int Hp = tiles_y * kT3H + 2 * F.G, Wp = S.tiles_x * kT3W + 2 * F.G;
+  S.pitch = (Wp + 7) / 8 * 8;
+  S.plane = (size_t)Hp * S.pitch;
+  const long long tiles = (long long)tiles_y * S.tiles_x;
+  if (tiles > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
+  int used = 0;
+  for (char u : pl.slot_used) used += u ? 1 : 0;
+  const size_t frame_bytes = S.plane * sizeof(float) * (18 + 10 * (size_t)used);
+  const size_t wtab_bytes = pl.wtab.size() * sizeof(float);
+  char* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, frame_bytes + wtab_bytes + 256, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(3x3 scratch)");
+  float* p = reinterpret_cast<float*>(scratch);
+  S.c18 = p;
+  p += 18 * S.plane;
+  for (size_t si = 0; si < pl.scales.size(); ++si)
+    if (pl.slot_used[si]) {
+      S.s9[si] = p;
+      p += 9 * S.plane;
+      S.ld[si] = p;
+      p += S.plane;
+    }
+  float* d_wtab = reinterpret_cast<float*>(scratch + (frame_bytes + 255) / 256 * 256);
+  S.out = cout;
+  e = cudaMemcpyAsync(d_wtab, pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice, st);
+  F.wtab = d_wtab;
+  F.n_scenes = 1;
+  F.total_tiles = (int)tiles;
+  if (e == cudaSuccess) {
+    dim3 blk(32, 8), grd((Wp + 31) / 32, (Hp + 7) / 8);
+    prep3_cov_kernel<<<grd, blk, 0, st>>>(cin, H, W, const_cast<float*>(S.c18), Hp, Wp, S.pitch, S.plane, F.G);
+    const float gamma = rescale_gamma_3x3();
+    for (size_t si = 0; si < pl.scales.size(); ++si) {
+      if (!pl.slot_used[si]) continue;
+      GaussArg ga;
+      std::memset(&ga, 0, sizeof ga);
+      const std::vector<float> gw = gauss_weights(pl.scales[si]);
+      std::copy(gw.begin(), gw.end(), ga.g);
+      prep3_scale_kernel<<<grd, blk, 0, st>>>(S.c18, Hp, Wp, S.pitch, S.plane, pl.scales[si], ga, gamma,
+                                              const_cast<float*>(S.s9[si]), const_cast<float*>(S.ld[si]));
+    }
+    static size_t configured = 0;
+    if (smem > configured) {
+      e = cudaFuncSetAttribute(nlsar3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) configured = smem;
+    }
+    if (e == cudaSuccess) {
+      nlsar3_kernel<<<(unsigned)tiles, kT3Threads, smem, st>>>(F, S);
+      e = cudaGetLastError();
+    }
+    profile_count(2 + used);
+  }
+  cudaFreeAsync(scratch, st);
+  if (e != cudaSuccess) return cuda_error(e, "NL-SAR 3x3");
+  return DCL_OK;
+}
+
+// Host pointers: copy in, run, copy out.
+int nlsar_covmat3_host(const Plan& pl, const float* cin, float* cout, int H, int W) {
+  if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  int dev = 0;
+  int rc = ensure_device_ready(dev);
+  if (rc) return rc;
+  cudaStream_t st = cudaStreamPerThread;
+  const size_t n = (size_t)18 * H * W, b = n * sizeof(float);
+  float* buf = nullptr;
+  cudaError_t e = cudaMallocAsync(&buf, 2 * b, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io)");
+  e = cudaMemcpyAsync(buf, cin, b, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(buf, st);
+    return cuda_error(e, "cudaMemcpyAsync(H2D)");
+  }
+  rc = nlsar_covmat3_device(pl, buf, buf + n, H, W, st);
+  if (rc == DCL_OK) {
+    e = cudaMemcpyAsync(cout, buf + n, b, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
+  }
+  cudaFreeAsync(buf, st);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR 3x3");
+  return rc;
+}
+
+namespace {
+
+struct DevMem {
+  void* p = nullptr;
+  ~DevMem() {
+    if (p) cudaFree(p);
+  }
+};
+
+int train3_one(const float* d_cov, int H, int W, int p, int s, std::vector<float>& sorted) {
+  const int Ho = H - s + 1, Wo = W - s + 1;
+  if (Ho < 1 || Wo < 1)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "training area %dx%d smaller than scale %d", H, W, s);
+  const int nh = (Ho + p - 1) / p, nw = (Wo + p - 1) / p;
+  const long long n = (long long)nh * nw;
+  if (n < 2) return set_error(DCL_ERR_INVALID_ARGUMENT, "training area holds fewer than two %dx%d patches", p, p);
+  const long long npairs = n * (n - 1) / 2;
+  const int pp = p * p;
+  DevMem avg, pat, dis, dis2;
+  cudaError_t e = cudaMalloc(&avg.p, (size_t)Ho * Wo * 9 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&pat.p, (size_t)n * pp * 9 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dis.p, (size_t)npairs * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dis2.p, (size_t)npairs * sizeof(float));
+  if (e != cudaSuccess) return cuda_error(e, "training buffers");
+  GaussArg ga;
+  std::memset(&ga, 0, sizeof ga);
+  const std::vector<float> g = gauss_weights(s);
+  std::copy(g.begin(), g.end(), ga.g);
+  dim3 blk(32, 8), grd((Wo + 31) / 32, (Ho + 7) / 8);
+  train3_avg_kernel<<<grd, blk>>>(d_cov, H, W, s, ga, rescale_gamma_3x3(), (float*)avg.p);
+  train3_gather_kernel<<<(unsigned)((n * pp + 255) / 256), 256>>>((const float*)avg.p, Ho, Wo, p, nw, (int)n,
+                                                                  (float*)pat.p);
+  train3_pairs_kernel<<<(unsigned)((npairs + 255) / 256), 256>>>((const float*)pat.p, pp, npairs,
+                                                                2 * 3 * std::log(2.0f), (float*)dis.p);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "training kernels");
+  return sort_dissims((float*)dis.p, (float*)dis2.p, npairs, sorted);
+}
+
+}  // namespace
+
+dcl_stats_collection* training_covmat3(const float* cov18, int H, int W, const int* patches, int np,
+                                       const int* scales, int ns) {
+  if (!cov18 || H < 1 || W < 1) {
+    set_error(DCL_ERR_INVALID_ARGUMENT, "null input or empty training area");
+    return nullptr;
+  }
+  if (!patches || !scales || np < 1 || ns < 1) {
+    set_error(DCL_ERR_INVALID_ARGUMENT, "patch_sizes and scale_sizes must not be empty");
+    return nullptr;
+  }
+  const size_t n = (size_t)18 * H * W;
+  DevMem d_cov;
+  cudaError_t e = cudaMalloc(&d_cov.p, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(d_cov.p, cov18, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cuda_error(e, "training setup");
+    return nullptr;
+  }
+  dcl_stats_collection* c = dcl_collection_new();
+  // get_stats.cpp:33-37: patch outer, scale inner; lut_size 256 (:31)
+  for (int pi = 0; pi < np; ++pi)
+    for (int si = 0; si < ns; ++si) {
+      const int p = patches[pi], s = scales[si];
+      if (p < 1 || p % 2 == 0 || s < 1 || s % 2 == 0 || s * s > kMaxGauss) {
+        set_error(DCL_ERR_INVALID_ARGUMENT, "patch and scale sizes must be odd (scale <= 9)");
+        dcl_stats_collection_free(c);
+        return nullptr;
+      }
+      std::vector<float> sorted;
+      if (train3_one((const float*)d_cov.p, H, W, p, s, sorted) != DCL_OK) {
+        dcl_stats_collection_free(c);
+        return nullptr;
+      }
+      dcl_collection_put(c, p, s, stats_from_sorted(sorted, 256));
+    }
+  return c;
+}
+
+}  // namespace dcl

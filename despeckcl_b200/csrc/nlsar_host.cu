@@ -591,12 +591,12 @@ extern "C" int dcl_nlsar_insar_device(const float* a1, const float* a2, const fl
 extern "C" int dcl_nlsar_covmat(const float* cin, float* cout, int H, int W, int dim, int sws, const int* patches,
                                 int np, const int* scales, int ns, const dcl_stats_entry* stats, int nstats, float h,
                                 float c, int select_mode) {
-  if (dim != 2)
-    return set_error(dim == 3 ? DCL_ERR_UNSUPPORTED : DCL_ERR_INVALID_ARGUMENT,
-                     "covariance dimension %d: only 2x2 (InSAR) covariances are supported", dim);
+  if (dim != 2 && dim != 3)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "covariance dimension %d: 2x2 and 3x3 covariances are supported", dim);
   Plan pl;
   int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, true, pl);
   if (rc) return rc;
+  if (dim == 3) return nlsar_covmat3_host(pl, cin, cout, H, W);
   return run_host_covmat(pl, cin, cout, H, W);
 }
 
@@ -604,13 +604,13 @@ extern "C" int dcl_nlsar_covmat_device(const float* cin, float* cout, int H, int
                                        const int* patches, int np, const int* scales, int ns,
                                        const dcl_stats_entry* stats, int nstats, float h, float c, int select_mode,
                                        void* stream) {
-  if (dim != 2)
-    return set_error(dim == 3 ? DCL_ERR_UNSUPPORTED : DCL_ERR_INVALID_ARGUMENT,
-                     "covariance dimension %d: only 2x2 (InSAR) covariances are supported", dim);
+  if (dim != 2 && dim != 3)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "covariance dimension %d: 2x2 and 3x3 covariances are supported", dim);
   if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   Plan pl;
   int rc = make_plan(sws, patches, np, scales, ns, stats, nstats, h, c, select_mode, true, pl);
   if (rc) return rc;
+  if (dim == 3) return nlsar_covmat3_device(pl, cin, cout, H, W, (cudaStream_t)stream);
   SceneIO s{nullptr, nullptr, nullptr, cin, nullptr, nullptr, nullptr, cout, nullptr, H, W};
   return run_device(pl, {s}, (cudaStream_t)stream);
 }

@@ -41,5 +41,9 @@ int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scene
                  int variant = 0);
 // whether the call is served by the specialised kernel (variants apply)
 bool uses_specialised_kernel(const Plan& pl);
+// NL-SAR of a 3x3 covariance scene [18][H][W] (nlsar_dim3.cu): device
+// pointers on `st`, or host pointers (copied in and out, synchronous)
+int nlsar_covmat3_device(const Plan& pl, const float* cin, float* cout, int H, int W, cudaStream_t st);
+int nlsar_covmat3_host(const Plan& pl, const float* cin, float* cout, int H, int W);
 
 }  // namespace dcl

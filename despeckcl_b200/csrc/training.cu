@@ -119,6 +119,27 @@ struct DevBuf {
 
 }  // namespace
 
+// Sorts the npairs device dissimilarities in `dis` (into `dis2`) and returns the
+// finite ones on the host, ascending (stats.cpp:28-38 drops NaN and inf).
+int sort_dissims(float* dis, float* dis2, long long npairs, std::vector<float>& sorted) {
+  DevBuf tmp;
+  size_t tmp_bytes = 0;
+  cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, (const float*)dis, dis2, (int)npairs);
+  cudaError_t e = cudaMalloc(&tmp.p, tmp_bytes);
+  if (e != cudaSuccess) return cuda_error(e, "training sort buffer");
+  e = cub::DeviceRadixSort::SortKeys(tmp.p, tmp_bytes, (const float*)dis, dis2, (int)npairs);
+  if (e != cudaSuccess) return cuda_error(e, "training sort");
+  std::vector<float> all((size_t)npairs);
+  e = cudaMemcpy(all.data(), dis2, all.size() * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_error(e, "training copy");
+  sorted.clear();
+  sorted.reserve(all.size());
+  for (float v : all)
+    if (std::isfinite(v)) sorted.push_back(v);
+  if (sorted.empty()) return set_error(DCL_ERR_INVALID_ARGUMENT, "no finite dissimilarity in the training area");
+  return DCL_OK;
+}
+
 // dissimilarities of one (patch, scale) on a device covariance image; returns
 // them sorted ascending, finite values only
 static int train_one(const float4* d_cov, int H, int W, int p, int s, std::vector<float>& sorted) {
@@ -130,7 +151,7 @@ static int train_one(const float4* d_cov, int H, int W, int p, int s, std::vecto
   if (n < 2) return set_error(DCL_ERR_INVALID_ARGUMENT, "training area holds fewer than two %dx%d patches", p, p);
   const long long npairs = n * (n - 1) / 2;
   const int pp = p * p;
-  DevBuf avg, pat, dis, dis2, tmp;
+  DevBuf avg, pat, dis, dis2;
   cudaError_t e = cudaMalloc(&avg.p, (size_t)Ho * Wo * sizeof(float4));
   if (e == cudaSuccess) e = cudaMalloc(&pat.p, (size_t)n * pp * sizeof(float4));
   if (e == cudaSuccess) e = cudaMalloc(&dis.p, (size_t)npairs * sizeof(float));
@@ -148,21 +169,7 @@ static int train_one(const float4* d_cov, int H, int W, int p, int s, std::vecto
                                                                2 * 2 * std::log(2.0f), (float*)dis.p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "training kernels");
-  size_t tmp_bytes = 0;
-  cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, (const float*)dis.p, (float*)dis2.p, (int)npairs);
-  e = cudaMalloc(&tmp.p, tmp_bytes);
-  if (e != cudaSuccess) return cuda_error(e, "training sort buffer");
-  e = cub::DeviceRadixSort::SortKeys(tmp.p, tmp_bytes, (const float*)dis.p, (float*)dis2.p, (int)npairs);
-  if (e != cudaSuccess) return cuda_error(e, "training sort");
-  std::vector<float> all((size_t)npairs);
-  e = cudaMemcpy(all.data(), dis2.p, all.size() * sizeof(float), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_error(e, "training copy");
-  sorted.clear();
-  sorted.reserve(all.size());
-  for (float v : all)
-    if (std::isfinite(v)) sorted.push_back(v);
-  if (sorted.empty()) return set_error(DCL_ERR_INVALID_ARGUMENT, "no finite dissimilarity in the training area");
-  return DCL_OK;
+  return sort_dissims((float*)dis.p, (float*)dis2.p, npairs, sorted);
 }
 
 static dcl_stats_collection* train_common(const float4* d_cov, int H, int W, const int* patches, int np,
@@ -226,9 +233,9 @@ extern "C" dcl_stats_collection* dcl_nlsar_training_insar(const float* a1, const
 
 extern "C" dcl_stats_collection* dcl_nlsar_training_covmat(const float* cov8, int H, int W, int dim,
                                                            const int* patches, int np, const int* scales, int ns) {
+  if (dim == 3) return training_covmat3(cov8, H, W, patches, np, scales, ns);
   if (dim != 2) {
-    set_error(dim == 3 ? DCL_ERR_UNSUPPORTED : DCL_ERR_INVALID_ARGUMENT,
-              "covariance dimension %d: only 2x2 (InSAR) covariances are supported", dim);
+    set_error(DCL_ERR_INVALID_ARGUMENT, "covariance dimension %d: 2x2 and 3x3 covariances are supported", dim);
     return nullptr;
   }
   if (!cov8 || H < 1 || W < 1) {

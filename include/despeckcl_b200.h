@@ -117,8 +117,9 @@ int dcl_nlsar_insar_device_noalloc(const float* ampl_master, const float* ampl_s
                                    void* stream);
 
 /* NL-SAR on a covariance image [2*dim*dim][height][width] (even planes real,
- * odd planes imaginary), host pointers.  dim 2 only (dim 3 returns
- * DCL_ERR_UNSUPPORTED).  Replaces despeckcl::nlsar (include/despeckcl.h:62-73). */
+ * odd planes imaginary), host pointers.  dim 2 (InSAR) or 3 (PolSAR); any
+ * other dim is DCL_ERR_INVALID_ARGUMENT.  Replaces despeckcl::nlsar
+ * (include/despeckcl.h:62-73). */
 int dcl_nlsar_covmat(const float* covmat_raw, float* covmat_filt, int height, int width, int dim,
                      int search_window_size, const int* patch_sizes, int n_patch_sizes, const int* scale_sizes,
                      int n_scale_sizes, const dcl_stats_entry* stats, int n_stats, float h_param, float c_param,
@@ -262,7 +263,7 @@ dcl_stats_collection* dcl_nlsar_training_insar(const float* ampl_master, const f
                                                const float* phase, int height, int width, const int* patch_sizes,
                                                int n_patch_sizes, const int* scale_sizes, int n_scale_sizes);
 
-/* Training on a covariance image [2*dim*dim][height][width]; dim 2 only.
+/* Training on a covariance image [2*dim*dim][height][width]; dim 2 or 3.
  * Replaces despeckcl::nlsar_training (include/despeckcl.h:85-92). */
 dcl_stats_collection* dcl_nlsar_training_covmat(const float* covmat, int height, int width, int dim,
                                                 const int* patch_sizes, int n_patch_sizes, const int* scale_sizes,

@@ -57,11 +57,14 @@ def test_argument_validation_happens_on_the_host(kw, code):
     assert e.value.code == code
 
 
-def test_covariance_dim3_is_reported_unsupported():
-    cov = np.zeros((3, 3, 4, 4), np.complex64)
+@pytest.mark.parametrize("dim", [1, 4])
+def test_covariance_dimension_outside_2_and_3_is_rejected(dim):
+    # 2x2 and 3x3 covariances are filtered; any other size is an invalid
+    # argument, reported before any device work
+    cov = np.zeros((dim, dim, 4, 4), np.complex64)
     with pytest.raises(dcl.DespeckclError) as e:
         dcl.nlsar(cov, 21, [3], [1], {(3, 1): _stats_entry(3, 1)})
-    assert e.value.code == -5
+    assert e.value.code == -1
 
 
 def test_lut_builder_matches_oracle(oracle):
