@@ -90,6 +90,107 @@ __global__ void __launch_bounds__(kBoxThreads)
   }
 }
 
+// Compile-time window radius R (w = 2R+1 <= 15): a 64 x 32 tile per CTA,
+// window sums from registers, each thread producing 4 consecutive outputs
+// (columns in the horizontal pass, rows in the vertical one) from 4 + 2R
+// loaded values per plane.  Every output sums its window left to right
+// (top to bottom) from 0, as the generic kernel does, so both give the same
+// bits.
+template <int R>
+__global__ void __launch_bounds__(kBoxThreads)
+    boxcar_r_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
+                    float* __restrict__ ref, float* __restrict__ phase, float* __restrict__ coh, int H, int W) {
+  constexpr int SW = kBoxTW + 2 * R, SH = kBoxTH + 2 * R, N = 4 + 2 * R;
+  extern __shared__ float sm[];
+  float* sIn = sm;                   // [3][SH][SW]: I, Re, Im
+  float* sHs = sm + 3 * SH * SW;     // [3][SH][kBoxTW] horizontal sums
+  const int vy0 = blockIdx.y * kBoxTH, vx0 = blockIdx.x * kBoxTW;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < SH * SW; i += kBoxThreads) {
+    const int rr = i / SW, cc = i - rr * SW;
+    const int y = clampi_b(vy0 - R + rr, 0, H - 1), x = clampi_b(vx0 - R + cc, 0, W - 1);
+    const size_t g = (size_t)y * W + x;
+    const float am = a1[g], as = a2[g];
+    float sn, cs;
+    __sincosf(phi[g], &sn, &cs);
+    const float aa = am * as;
+    sIn[i] = (am * am + as * as) / 2;
+    sIn[SH * SW + i] = aa * cs;
+    sIn[2 * SH * SW + i] = aa * sn;
+  }
+  __syncthreads();
+  // horizontal: item = (plane, row, group of 4 columns)
+  constexpr int HG = kBoxTW / 4;
+  for (int it = tid; it < 3 * SH * HG; it += kBoxThreads) {
+    const int pl = it / (SH * HG);
+    const int rem = it - pl * SH * HG;
+    const int rr = rem / HG, c0 = (rem - rr * HG) * 4;
+    const float* src = sIn + pl * SH * SW + rr * SW + c0;
+    float v[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = src[k];
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float acc = 0.f;
+#pragma unroll
+      for (int k = 0; k <= 2 * R; ++k) acc += v[q + k];
+      o[q] = acc;
+    }
+    *reinterpret_cast<float4*>(sHs + pl * SH * kBoxTW + rr * kBoxTW + c0) = make_float4(o[0], o[1], o[2], o[3]);
+  }
+  __syncthreads();
+  // vertical: item = (group of 4 rows, column); all three planes
+  const float inv_n = 1.0f / (float)((2 * R + 1) * (2 * R + 1));
+  for (int it = tid; it < (kBoxTH / 4) * kBoxTW; it += kBoxThreads) {
+    const int r0 = (it / kBoxTW) * 4, cc = it - (it / kBoxTW) * kBoxTW;
+    float sum[3][4];
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) {
+      const float* src = sHs + pl * SH * kBoxTW + r0 * kBoxTW + cc;
+      float v[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) v[k] = src[k * kBoxTW];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k <= 2 * R; ++k) acc += v[q + k];
+        sum[pl][q] = acc;
+      }
+    }
+    const int vx = vx0 + cc;
+    const int ox = (vx < W - 1) ? vx : (vx == W - 1 + R ? W - 1 : -1);
+    if (ox < 0) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int vy = vy0 + r0 + q;
+      const int oy = (vy < H - 1) ? vy : (vy == H - 1 + R ? H - 1 : -1);
+      if (oy < 0) continue;
+      const float si = sum[0][q], sr = sum[1][q], sj = sum[2][q];
+      const size_t o = (size_t)oy * W + ox;
+      ref[o] = si * inv_n;
+      phase[o] = atan2f(sj, sr);
+      coh[o] = sqrtf(sr * sr + sj * sj) / si;
+    }
+  }
+}
+
+template <int R>
+cudaError_t launch_boxcar_r(const float* a1, const float* a2, const float* phi, float* ref, float* phase, float* coh,
+                            int H, int W, dim3 grid, cudaStream_t st) {
+  constexpr size_t smem = (size_t)3 * ((kBoxTH + 2 * R) * (kBoxTW + 2 * R) + (kBoxTH + 2 * R) * kBoxTW) * 4;
+  static bool configured = false;
+  if (smem > 48 * 1024 && !configured) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(boxcar_r_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  boxcar_r_kernel<R><<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 int boxcar_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase, float* coh, int H,
@@ -103,14 +204,26 @@ int boxcar_device(const float* a1, const float* a2, const float* phi, float* ref
   dim3 grid((vW + kBoxTW) / kBoxTW, (vH + kBoxTH) / kBoxTH);
   const size_t smem = (size_t)3 * ((kBoxTH + 2 * r) * (kBoxTW + 2 * r) + (kBoxTH + 2 * r) * kBoxTW) * sizeof(float);
   static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
+  if (r > 7 && smem > 48 * 1024 && smem > configured) {
     cudaError_t e = cudaFuncSetAttribute(boxcar_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(boxcar)");
     configured = smem;
   }
-  boxcar_kernel<<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W, r);
+  cudaError_t e = cudaSuccess;
+  switch (r) {
+    case 0: e = launch_boxcar_r<0>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 1: e = launch_boxcar_r<1>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 2: e = launch_boxcar_r<2>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 3: e = launch_boxcar_r<3>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 4: e = launch_boxcar_r<4>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 5: e = launch_boxcar_r<5>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 6: e = launch_boxcar_r<6>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    case 7: e = launch_boxcar_r<7>(a1, a2, phi, ref, phase, coh, H, W, grid, st); break;
+    default:
+      boxcar_kernel<<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W, r);
+      e = cudaGetLastError();
+  }
   profile_count(1);
-  const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "boxcar launch");
   return DCL_OK;
 }

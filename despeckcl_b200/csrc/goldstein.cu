@@ -23,7 +23,7 @@
 //     |Z|^alpha (weighted_multiply.cl), transforms back with the 1/p^2 scale
 //     of the reference's clFFT plan (goldstein_patch_ft_test.cpp) and stores the
 //     patch;
-//  goldstein_pack_kernel   one thread per output pixel: the raw interferogram
+//  goldstein_pack_kernel   one thread per 4 output pixels of a row: the raw interferogram
 //     plus the weighted contributions of the (up to four) patches covering the
 //     pixel, added in the order of the reference's four parity launches, which
 //     accumulate onto the buffer that still holds the raw interferogram
@@ -202,45 +202,28 @@ __device__ __forceinline__ float pack_factor(int rel, int o, int ov, int sub) {
   return f;
 }
 
+constexpr int kPackX = 4;  // output columns per thread (32 apart: coalesced per warp)
+
 __global__ void __launch_bounds__(256)
     goldstein_pack_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
                           const float2* __restrict__ patches, float* __restrict__ ref, float* __restrict__ phase,
                           GoldsteinGeom g, GoldsteinTile t) {
-  const int x = t.x_lo + blockIdx.x * 32 + (threadIdx.x & 31);
   const int y = t.y_lo + blockIdx.y * 8 + (threadIdx.x >> 5);
-  if (x > t.x_hi || y > t.y_hi) return;
+  if (y > t.y_hi) return;
   // tile position whose result lands here (the clamped write-back keeps the
   // last one; only the last tile row / column reaches row H-1 / column W-1)
   const int ty = (y == g.H - 1) ? g.sub - g.ov - 1 : y - t.h0;
-  const int tx = (x == g.W - 1) ? g.sub - g.ov - 1 : x - t.w0;
-  float2 v;
-  {
-    const size_t i = (size_t)clampg(t.h0 + ty, 0, g.H - 1) * g.W + clampg(t.w0 + tx, 0, g.W - 1);
-    const float amp = 0.5f * (a1[i] + a2[i]);
-    float sn, cs;
-    __sincosf(phi[i], &sn, &cs);
-    v = make_float2(amp * cs, amp * sn);
-  }
+  const size_t irow = (size_t)clampg(t.h0 + ty, 0, g.H - 1) * g.W;
   // covering patches per axis: q = (t + ov) / s at offset t + ov - q s, and
-  // q - 1 at offset + s when that is still inside the patch (one of each parity)
-  const int qx = div_s(tx + g.ov, g), cx = tx + g.ov - qx * g.s;
+  // q - 1 at offset + s when that is still inside the patch (one of each
+  // parity); index 0 of the arrays below is the even patch, 1 the odd one
   const int qy = div_s(ty + g.ov, g), ry = ty + g.ov - qy * g.s;
-  // candidate 0: patch q, candidate 1: patch q - 1; e = the even one
-  const bool vx0 = qx >= t.px_lo && qx < t.px_lo + t.n_px;
-  const bool vx1 = qx - 1 >= t.px_lo && qx - 1 < t.px_lo + t.n_px && cx + g.s < kP;
   const bool vy0 = qy >= t.py_lo && qy < t.py_lo + t.n_py;
   const bool vy1 = qy - 1 >= t.py_lo && qy - 1 < t.py_lo + t.n_py && ry + g.s < kP;
-  const bool xe1 = qx & 1, ye1 = qy & 1;  // the even patch is candidate 1
-  int px_[2], cx_[2], py_[2], ry_[2];
-  bool vx_[2], vy_[2];
-  float fx_[2], fy_[2];
-  // index 0: even parity, 1: odd parity
-  px_[0] = xe1 ? qx - 1 : qx;
-  px_[1] = xe1 ? qx : qx - 1;
-  cx_[0] = xe1 ? cx + g.s : cx;
-  cx_[1] = xe1 ? cx : cx + g.s;
-  vx_[0] = xe1 ? vx1 : vx0;
-  vx_[1] = xe1 ? vx0 : vx1;
+  const bool ye1 = qy & 1;
+  int py_[2], ry_[2];
+  bool vy_[2];
+  float fy_[2];
   py_[0] = ye1 ? qy - 1 : qy;
   py_[1] = ye1 ? qy : qy - 1;
   ry_[0] = ye1 ? ry + g.s : ry;
@@ -248,25 +231,52 @@ __global__ void __launch_bounds__(256)
   vy_[0] = ye1 ? vy1 : vy0;
   vy_[1] = ye1 ? vy0 : vy1;
 #pragma unroll
-  for (int a = 0; a < 2; ++a) {
-    fx_[a] = pack_factor(cx_[a], tx, g.ov, g.sub);
-    fy_[a] = pack_factor(ry_[a], ty, g.ov, g.sub);
-  }
-  // the reference's four parity launches in order: (x, y) parity (0,0), (0,1), (1,0), (1,1)
+  for (int b = 0; b < 2; ++b) fy_[b] = pack_factor(ry_[b], ty, g.ov, g.sub);
+  const int x0 = t.x_lo + blockIdx.x * (32 * kPackX) + (threadIdx.x & 31);
 #pragma unroll
-  for (int xpar = 0; xpar < 2; ++xpar)
-#pragma unroll
-    for (int ypar = 0; ypar < 2; ++ypar) {
-      if (!vx_[xpar] || !vy_[ypar]) continue;
-      const float f = fx_[xpar] * fy_[ypar];
-      const float2 q = patches[((size_t)(py_[ypar] - t.py_lo) * t.n_px + (px_[xpar] - t.px_lo)) * kP * kP +
-                               ry_[ypar] * kP + cx_[xpar]];
-      v.x += f * q.x;
-      v.y += f * q.y;
+  for (int m = 0; m < kPackX; ++m) {
+    const int x = x0 + 32 * m;
+    if (x > t.x_hi) break;
+    const int tx = (x == g.W - 1) ? g.sub - g.ov - 1 : x - t.w0;
+    float2 v;
+    {
+      const size_t i = irow + clampg(t.w0 + tx, 0, g.W - 1);
+      const float amp = 0.5f * (a1[i] + a2[i]);
+      float sn, cs;
+      __sincosf(phi[i], &sn, &cs);
+      v = make_float2(amp * cs, amp * sn);
     }
-  const size_t o = (size_t)y * g.W + x;
-  ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
-  phase[o] = atan2f(v.y, v.x);
+    const int qx = div_s(tx + g.ov, g), cx = tx + g.ov - qx * g.s;
+    const bool vx0 = qx >= t.px_lo && qx < t.px_lo + t.n_px;
+    const bool vx1 = qx - 1 >= t.px_lo && qx - 1 < t.px_lo + t.n_px && cx + g.s < kP;
+    const bool xe1 = qx & 1;
+    int px_[2], cx_[2];
+    bool vx_[2];
+    float fx_[2];
+    px_[0] = xe1 ? qx - 1 : qx;
+    px_[1] = xe1 ? qx : qx - 1;
+    cx_[0] = xe1 ? cx + g.s : cx;
+    cx_[1] = xe1 ? cx : cx + g.s;
+    vx_[0] = xe1 ? vx1 : vx0;
+    vx_[1] = xe1 ? vx0 : vx1;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) fx_[a] = pack_factor(cx_[a], tx, g.ov, g.sub);
+    // the reference's four parity launches in order: (x, y) parity (0,0), (0,1), (1,0), (1,1)
+#pragma unroll
+    for (int xpar = 0; xpar < 2; ++xpar)
+#pragma unroll
+      for (int ypar = 0; ypar < 2; ++ypar) {
+        if (!vx_[xpar] || !vy_[ypar]) continue;
+        const float f = fx_[xpar] * fy_[ypar];
+        const float2 q = patches[((size_t)(py_[ypar] - t.py_lo) * t.n_px + (px_[xpar] - t.px_lo)) * kP * kP +
+                                 ry_[ypar] * kP + cx_[xpar]];
+        v.x += f * q.x;
+        v.y += f * q.y;
+      }
+    const size_t o = (size_t)y * g.W + x;
+    ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
+    phase[o] = atan2f(v.y, v.x);
+  }
 }
 
 // patches (of the n per side) covering tile positions [lo, hi]
@@ -353,7 +363,7 @@ int goldstein_device(const float* a1, const float* a2, const float* phi, float* 
     const size_t n = (size_t)t.n_py * t.n_px;
     goldstein_patch_kernel<<<(unsigned)((n + kWarps - 1) / kWarps), 32 * kWarps, 0, st>>>(a1, a2, phi, patches, g, t,
                                                                                          alpha);
-    dim3 grid((t.x_hi - t.x_lo + 32) / 32, (t.y_hi - t.y_lo + 8) / 8);
+    dim3 grid((t.x_hi - t.x_lo + 32 * kPackX) / (32 * kPackX), (t.y_hi - t.y_lo + 8) / 8);
     goldstein_pack_kernel<<<grid, 256, 0, st>>>(a1, a2, phi, patches, ref, phase, g, t);
     profile_count(2);
   }
