@@ -59,6 +59,31 @@ def parse():
     return p.parse_args()
 
 
+def max_over_ranks(value, dist, device):
+    """The largest `value` over all ranks, returned on every rank (`value`
+    itself without a process group).  Times of a multi-GPU run are reported
+    as the maximum over ranks."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank):
+    """Scene seed of a replica: each rank filters its own scene (weak scaling,
+    no data exchanged between ranks)."""
+    return 1 + rank
+
+
+def aggregate_mpix(n_ranks, side, ms):
+    """Whole-job Mpix/s: every rank filtered one side x side scene in `ms`
+    (the slowest rank's time)."""
+    return n_ranks * side * side / (ms * 1e-3) / 1e6
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -212,7 +237,7 @@ def run_ours(args):
     L = dcl.lib()
     S = args.size
     stats = make_stats(dcl, synthetic)
-    a1, a2, ph = synthetic.insar_scene(S, S, 1 + rank)
+    a1, a2, ph = synthetic.insar_scene(S, S, replica_seed(rank))
     dev = [torch.from_numpy(x).cuda() for x in (a1, a2, ph)]
     out = tuple(torch.empty((S, S), dtype=torch.float32, device="cuda") for _ in range(3))
     stream = torch.cuda.current_stream()
@@ -241,14 +266,11 @@ def run_ours(args):
         rc = L.dcl_profile_end(ctypes.byref(fused_ms), ctypes.byref(fused_n), ctypes.byref(all_n))
         if rc != 0:
             raise RuntimeError(L.dcl_last_error().decode())
-    ms_step = start.elapsed_time(stop) / args.steps
+    ms_step = max_over_ranks(start.elapsed_time(stop) / args.steps, dist, "cuda")
     if dist:
-        t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
         dist.barrier()
     clocks = clk.summary()
-    value = args.gpus * S * S / (ms_step * 1e-3) / 1e6
+    value = aggregate_mpix(args.gpus, S, ms_step)
 
     # end to end through the public host API, pinned host buffers
     pin = [torch.from_numpy(x).pin_memory() for x in (a1, a2, ph)]
@@ -273,12 +295,8 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(ke):
         e2e_step()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / ke
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = args.gpus * S * S / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / ke, dist, "cuda")
+    e2e_value = aggregate_mpix(args.gpus, S, e2e_ms)
     np.testing.assert_array_equal(hres[0], out[0].cpu().numpy())  # same result through both entry points
 
     peak = ctypes.c_double()

@@ -180,13 +180,9 @@ template <int R>
 cudaError_t launch_boxcar_r(const float* a1, const float* a2, const float* phi, float* ref, float* phase, float* coh,
                             int H, int W, dim3 grid, cudaStream_t st) {
   constexpr size_t smem = (size_t)3 * ((kBoxTH + 2 * R) * (kBoxTW + 2 * R) + (kBoxTH + 2 * R) * kBoxTW) * 4;
-  static bool configured = false;
-  if (smem > 48 * 1024 && !configured) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(boxcar_r_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  static size_t allowed[kMaxDevices];
+  const cudaError_t e = allow_dynamic_smem((const void*)boxcar_r_kernel<R>, smem, allowed);
+  if (e != cudaSuccess) return e;
   boxcar_r_kernel<R><<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W);
   return cudaGetLastError();
 }
@@ -203,11 +199,10 @@ int boxcar_device(const float* a1, const float* a2, const float* phi, float* ref
   const int vH = H - 1 + r, vW = W - 1 + r;
   dim3 grid((vW + kBoxTW) / kBoxTW, (vH + kBoxTH) / kBoxTH);
   const size_t smem = (size_t)3 * ((kBoxTH + 2 * r) * (kBoxTW + 2 * r) + (kBoxTH + 2 * r) * kBoxTW) * sizeof(float);
-  static size_t configured = 0;
-  if (r > 7 && smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(boxcar_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(boxcar)");
-    configured = smem;
+  static size_t allowed[kMaxDevices];
+  if (r > 7) {
+    const cudaError_t e = allow_dynamic_smem((const void*)boxcar_kernel, smem, allowed);
+    if (e != cudaSuccess) return cuda_error(e, "boxcar shared-memory limit");
   }
   cudaError_t e = cudaSuccess;
   switch (r) {

@@ -12,6 +12,12 @@ int cuda_error(cudaError_t e, const char* where);
 // Current device, its stream-ordered pool set to keep freed scratch between
 // calls (once per device).
 int ensure_device_ready(int& dev);
+// Devices a process may use (per-device caches are sized by it).
+constexpr int kMaxDevices = 64;
+// Allows `func` up to `bytes` of dynamic shared memory on the current device
+// (the limit is a per-device attribute); `cache` holds, per device, the
+// largest size already allowed, so repeated launches skip the call.
+cudaError_t allow_dynamic_smem(const void* func, size_t bytes, size_t* cache);
 // Count `n` kernel launches of the calling thread while dcl_profile_begin is active.
 void profile_count(int n);
 

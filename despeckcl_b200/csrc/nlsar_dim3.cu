@@ -515,11 +515,8 @@ int nlsar_covmat3_device(const Plan& pl0, const float* cin, float* cout, int H, 
       prep3_scale_kernel<<<grd, blk, 0, st>>>(S.c18, Hp, Wp, S.pitch, S.plane, pl.scales[si], ga, gamma,
                                               const_cast<float*>(S.s9[si]), const_cast<float*>(S.ld[si]));
     }
-    static size_t configured = 0;
-    if (smem > configured) {
-      e = cudaFuncSetAttribute(nlsar3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) configured = smem;
-    }
+    static size_t allowed[kMaxDevices];
+    e = allow_dynamic_smem((const void*)nlsar3_kernel, smem, allowed);
     if (e == cudaSuccess) {
       nlsar3_kernel<<<(unsigned)tiles, kT3Threads, smem, st>>>(F, S);
       e = cudaGetLastError();

@@ -26,6 +26,7 @@
 
 #include <cuda_runtime.h>
 
+#include "dcl_internal.h"
 #include "nlsar_common.cuh"
 
 namespace dcl {
@@ -400,13 +401,9 @@ template <int WSH, int PH0, int PH1, int PH2, int PX_>
 cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
   using C = Fast<WSH, PH0, PH1, PH2, PX_>;
   const size_t smem = (size_t)C::WORDS * 4;
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  static size_t allowed[kMaxDevices];
+  const cudaError_t e = allow_dynamic_smem((const void*)nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_>, smem, allowed);
+  if (e != cudaSuccess) return e;
   nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
   return cudaGetLastError();
 }

@@ -333,6 +333,19 @@ static const bool g_force_generic = [] {
   return s && s[0] == '1';
 }();
 
+cudaError_t allow_dynamic_smem(const void* func, size_t bytes, size_t* cache) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (bytes <= cache[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cache[dev] = bytes;
+  return e;
+}
+
 void profile_count(int n) {
   if (g_prof.on) g_prof.launches += n;
 }

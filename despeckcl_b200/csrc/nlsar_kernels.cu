@@ -32,6 +32,7 @@
 
 #include <cuda_runtime.h>
 
+#include "dcl_internal.h"
 #include "nlsar_common.cuh"
 
 namespace dcl {
@@ -421,21 +422,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Launch of the fused kernel (kept in this translation unit with the template).
 cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, int grid,
                                cudaStream_t st) {
-  static size_t configured[2] = {0, 0};  // largest dynamic size already allowed per instantiation
+  static size_t allowed8[kMaxDevices], allowed4[kMaxDevices];
   cudaError_t e = cudaSuccess;
   if (full8) {
-    if (smem > configured[1]) {
-      e = cudaFuncSetAttribute(nlsar_fused_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      configured[1] = smem;
-    }
+    e = allow_dynamic_smem((const void*)nlsar_fused_kernel<2, true>, smem, allowed8);
+    if (e != cudaSuccess) return e;
     nlsar_fused_kernel<2, true><<<grid, kThreads, smem, st>>>(F, d_scenes);
   } else {
-    if (smem > configured[0]) {
-      e = cudaFuncSetAttribute(nlsar_fused_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      configured[0] = smem;
-    }
+    e = allow_dynamic_smem((const void*)nlsar_fused_kernel<4, false>, smem, allowed4);
+    if (e != cudaSuccess) return e;
     nlsar_fused_kernel<4, false><<<grid, kThreads, smem, st>>>(F, d_scenes);
   }
   return cudaGetLastError();
