@@ -217,7 +217,10 @@ extern "C" dcl_nlsar_batch* dcl_nlsar_batch_create(int n, const float* const* a1
   for (int i = 0; i < n; ++i) {
     SceneDesc& d = b->desc[i];
     std::memset(&d, 0, sizeof d);
-    carve_scene(b->pl, b->geo[i], b->scratch + offs[i], d);
+    if (carve_scene(b->pl, b->geo[i], b->scratch + offs[i], d) != DCL_OK) {
+      release(b);
+      return nullptr;
+    }
     d.ref = ref[i];
     d.phase = phase[i];
     d.coh = coh[i];

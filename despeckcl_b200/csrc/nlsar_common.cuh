@@ -1,6 +1,7 @@
 // Shared host/device definitions of the fused NL-SAR engine.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -38,6 +39,11 @@ struct PassParams {
 // One scene of a (possibly batched) launch.  All padded arrays share one
 // frame: frame index = virtual coordinate + G, row pitch `pitch` elements.
 struct SceneDesc {
+  // TMA descriptors for the specialised kernel's staging: 2-D float views
+  // [Hp][4 pitch] of the cori and cs[s] frames with the boxes of one tile's
+  // staged regions; zero when that kernel is not used
+  CUtensorMap tm_co;
+  CUtensorMap tm_cs[kMaxScales];
   const float4* cori;   // un-rescaled covariance {C00, C11, Re C01, Im C01}
   const float4* cori2;  // covariance path only: {Im C00, Re C10, Im C10, Im C11}
   const float4* cs[kMaxScales];  // rescaled + Gaussian-averaged {C00, C11, Re C01, Im C01}
@@ -125,9 +131,24 @@ __global__ void prep_scale_kernel(const float4* cori, int Hp, int Wp, int pitch,
 cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, int grid,
                                cudaStream_t st);
 
+// Staged regions of the specialised kernel's tile (32 x 32 outputs), in
+// pixels: scaled covariance RS x RS, original covariance RO x RO.
+struct FastStage {
+  int RS, RO;
+};
+__host__ __device__ inline FastStage fast_stage(int wsh, int phm) {
+  FastStage f;
+  f.RS = 32 + 2 * (phm + wsh);
+  f.RO = 32 + 2 * wsh;
+  return f;
+}
+
 // The compile-time specialised kernel (nlsar_fast.cu) for the common
 // configurations; fast_kernel_supported() tells whether `F` has one.
 bool fast_kernel_supported(const FilterParams& F);
+// CTAs of the specialised kernel that gave up waiting for a staging copy
+// since the last call (the count is reset); 0 on success, -1 on a CUDA error
+int take_stage_timeouts(int* count);
 cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
                               int variant = 0);
 

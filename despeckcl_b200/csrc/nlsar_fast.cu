@@ -26,6 +26,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "dcl_internal.h"
 #include "nlsar_common.cuh"
 
@@ -55,20 +57,81 @@ struct Fast {
   static constexpr int HPL = K * SIMW * HP;         // one patch size's horizontal-sum plane
   static constexpr int LUTREP = 16;                 // interleaved LUT copies: two lanes per copy
   // shared memory, in 4-byte words
+  // the two TMA destinations start on 128-byte boundaries
   static constexpr int OFF_CS = 0;
-  static constexpr int OFF_CO = OFF_CS + 4 * RS * RS;
+  static constexpr int OFF_CO = (OFF_CS + 4 * RS * RS + 31) / 32 * 32;
   static constexpr int OFF_H = OFF_CO + 4 * RO * RO;
   static constexpr int OFF_LD = OFF_H + NP * HPL;
   static constexpr int OFF_SIM = OFF_LD + RS * RS;
   static constexpr int OFF_LUT = OFF_SIM + K * SIMW * SIMP;
-  static constexpr int WORDS = OFF_LUT + NP * kMaxLut * LUTREP;
+  static constexpr int OFF_BAR = (OFF_LUT + NP * kMaxLut * LUTREP + 1) / 2 * 2;  // the mbarrier (8 bytes)
+  static constexpr int WORDS = OFF_BAR + 2;
+  static constexpr uint32_t CO_BYTES = 16u * RO * RO;  // one TMA box each
+  static constexpr uint32_t CS_BYTES = 16u * RS * RS;
   static_assert(SWS % K == 0, "offset batches must tile a window row");
   static_assert(PH0 >= 0, "at least one patch");
   static_assert(PX % 2 == 0, "pixels are accumulated in pairs");
   static_assert(SIMP % 8 == 0 && SIMP >= 4 * 7 + 4 * NQ4, "phase-B segments must stay inside a row");
   static_assert(HP >= TW && HP % 4 == 0, "horizontal-sum pitch");
   static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
+  static_assert(4 * RS <= 256 && 4 * RO <= 256, "TMA box sides are at most 256 elements");
 };
+
+// ---- TMA staging through one mbarrier --------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  // make the initialised barrier visible to the asynchronous (TMA) proxy
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// 2-D tiled copy of one box of `map` at (x, y) (in elements; x a multiple of
+// 4 floats) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Staging waits are bounded: a copy that has not landed after this many
+// polls (each a hardware-bounded suspension) is reported, not waited for.
+constexpr int kStageWaitPolls = 1 << 22;
+__device__ int g_stage_timeouts;  // CTAs that gave up waiting for a staging copy
+
+// Waits for phase `parity` of `bar` on every thread; false (for every thread
+// of the CTA) when any thread gave up.
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity) {
+  bool ok = false;
+  for (int i = 0; i < kStageWaitPolls && !ok; ++i) ok = mbar_try_wait(bar, parity);
+  const bool failed = __syncthreads_or(!ok) != 0;
+  if (failed && threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1);
+  return !failed;
+}
+
+// ln det of a staged scaled covariance, rounded like the prep kernel's
+// (sim_measures.h:31-34)
+__device__ __forceinline__ float ln_det(const float4 c) {
+  return logf(__fsub_rn(__fmul_rn(c.x, c.y), __fadd_rn(__fmul_rn(c.z, c.z), __fmul_rn(c.w, c.w))));
+}
 
 __device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 b, float lb, float c2d) {
   // sim_measures.h:52-64 with nlooks 1 and the per-pixel ln det precomputed:
@@ -97,8 +160,9 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
   constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RO = C::RO;
   constexpr int SIMW = C::SIMW, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
   constexpr int NT = C::THREADS, NW = C::WARPS;
-  extern __shared__ float4 smem4[];
+  extern __shared__ __align__(128) float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::OFF_BAR);
   float4* sCs = reinterpret_cast<float4*>(smem + C::OFF_CS);
   float4* sCo = reinterpret_cast<float4*>(smem + C::OFF_CO);
   float* sH = smem + C::OFF_H;  // [NP][K][SIMW][HP]
@@ -108,6 +172,9 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int y0 = warp * PX;
   const float c2d = P.c2d;
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  uint32_t parity = 0;
 
   for (int tile = blockIdx.x; tile < P.total_tiles; tile += gridDim.x) {
     int lo = 0, hi = P.n_scenes - 1;
@@ -121,11 +188,21 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
     const int vy0 = ty * C::TH, vx0 = tx * TW;
     const int G = P.G, pitch = S.pitch;
 
+    (void)pitch;
+    // stage the original covariance (tile + search halo) and the first
+    // pass's scaled covariance (tile + patch and search halo) with TMA; the
+    // barrier orders every thread's reads of the previous tile before the
+    // copies overwrite shared memory
     __syncthreads();
-    for (int i = tid; i < RO * RO; i += NT) {
-      const int r = i / RO, c = i - r * RO;
-      sCo[i] = S.cori[(size_t)(vy0 - WSH + r + G) * pitch + (vx0 - WSH + c + G)];
+    if (tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(bar, C::CO_BYTES + C::CS_BYTES);
+      tma_load_2d(sCo, &S.tm_co, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
+      tma_load_2d(sCs, &S.tm_cs[P.pass[0].scale_slot], 4 * (vx0 - PHM - WSH + G), vy0 - PHM - WSH + G, bar);
     }
+    if (!stage_wait(bar, parity)) return;
+    parity ^= 1u;
+    for (int i = tid; i < RS * RS; i += NT) sLd[i] = ln_det(sCs[i]);
 
     float2 acc[PX / 2][NP][8];  // .x: pixel 2i, .y: pixel 2i+1
     float best_e[PX], best_a[PX], best_s0[PX], best_m[PX][4];
@@ -141,31 +218,19 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       for (int d = 0; d < 4; ++d) best_m[i][d] = 0.f;
     }
 
-    // phase-A items of this thread (fixed for the whole launch): the
-    // similarity-map position it = tid + m NT, as an index into the scaled
-    // covariance region, or -1 past the map or in a row's padding
-    constexpr int A_ITEMS = (SIMW * SIMP + NT - 1) / NT;
-    int a_ci[A_ITEMS];
-#pragma unroll
-    for (int m = 0; m < A_ITEMS; ++m) {
-      const int it = tid + m * NT;
-      const int r = it / SIMP, c = it - (it / SIMP) * SIMP;
-      a_ci[m] = (it < SIMW * SIMP && c < SIMW) ? (r + WSH) * RS + (c + WSH) : -1;
-    }
-    int loaded_slot = -1;
+    int loaded_slot = P.pass[0].scale_slot;
     for (int ps = 0; ps < P.npass; ++ps) {
       const PassParams& pp = P.pass[ps];
       __syncthreads();
       if (pp.scale_slot != loaded_slot) {
-        const float4* cs = S.cs[pp.scale_slot];
-        const float* ldp = S.ld[pp.scale_slot];
-        const int by = vy0 - PHM - WSH + G, bx = vx0 - PHM - WSH + G;
-        for (int i = tid; i < RS * RS; i += NT) {
-          const int r = i / RS, c = i - r * RS;
-          const size_t g = (size_t)(by + r) * pitch + (bx + c);
-          sCs[i] = cs[g];
-          sLd[i] = ldp[g];
+        if (tid == 0) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_expect_tx(bar, C::CS_BYTES);
+          tma_load_2d(sCs, &S.tm_cs[pp.scale_slot], 4 * (vx0 - PHM - WSH + G), vy0 - PHM - WSH + G, bar);
         }
+        if (!stage_wait(bar, parity)) return;
+        parity ^= 1u;
+        for (int i = tid; i < RS * RS; i += NT) sLd[i] = ln_det(sCs[i]);
         loaded_slot = pp.scale_slot;
       }
       // composite weight tables, LUTREP interleaved copies
@@ -200,11 +265,11 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
           // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
           // thread and consecutive pixels on consecutive lanes (conflict free)
           // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-#pragma unroll
-          for (int m = 0; m < A_ITEMS; ++m) {
-            const int it = tid + m * NT;
-            const int ci = a_ci[m];
-            if (ci < 0) continue;
+          for (int it = tid; it < SIMW * SIMP; it += NT) {
+            const int r = it / SIMP;
+            const int c = it - r * SIMP;
+            if (c >= SIMW) continue;
+            const int ci = (r + WSH) * RS + (c + WSH);
             const float4 a = sCs[ci];
             const float la = sLd[ci];
             const int ni = ci + dy * RS + dx0;
@@ -420,6 +485,19 @@ cudaError_t launch_fast_px(const FilterParams& F, const SceneDesc* d_scenes, int
 }
 
 }  // namespace
+
+// Number of CTAs that gave up waiting for a TMA staging copy since the last
+// call (and resets it).  Their tiles were left unwritten.
+int take_stage_timeouts(int* count) {
+  int n = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&n, g_stage_timeouts, sizeof n);
+  if (e == cudaSuccess && n != 0) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof zero);
+  }
+  *count = n;
+  return e == cudaSuccess ? 0 : -1;
+}
 
 // Specialisations available: the search window 21 (half 10) with every pass
 // holding the patch halves {1,2,3} (patches 3,5,7) or the single half 1, 2 or

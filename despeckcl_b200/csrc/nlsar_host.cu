@@ -286,8 +286,49 @@ size_t scratch_bytes(const Plan& pl, const SceneGeom& g) {
   return b;
 }
 
-// Carve the scratch of one scene and fill its descriptor (pointers into `base`).
-void carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d) {
+// cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
+// link against libcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// A 2-D float tensor map: `inner` floats per row, `rows` rows, row stride
+// `stride` bytes, box `box_inner` x `box_rows`.  The constraints of the TMA
+// unit are checked here: base 16-byte aligned, stride a multiple of 16
+// bytes, box inner extent a multiple of 16 bytes, box sides at most 256.
+static int encode_map_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint64_t stride,
+                         uint32_t box_inner, uint32_t box_rows) {
+  EncodeTiledFn fn = encode_tiled_fn();
+  if (!fn) return set_error(DCL_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (stride & 15) || ((box_inner * 4) & 15) || box_inner > 256 ||
+      box_rows > 256 || box_inner > inner || box_rows > rows)
+    return set_error(DCL_ERR_INVALID_ARGUMENT, "TMA map: misaligned frame or box");
+  const cuuint64_t dims[2] = {inner, rows};
+  const cuuint64_t strides[1] = {stride};
+  const cuuint32_t box[2] = {box_inner, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(DCL_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return DCL_OK;
+}
+
+// Carve the scratch of one scene and fill its descriptor (pointers into
+// `base`, and the TMA maps of the specialised kernel when the plan uses it).
+int carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d) {
   const size_t plane = (size_t)g.Hp * g.pitch;
   char* p = base;
   d.cori = reinterpret_cast<float4*>(p);
@@ -315,6 +356,19 @@ void carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d) {
   d.pitch = g.pitch;
   d.tiles_x = g.tiles_x;
   d.tiles_y = g.tiles_y;
+  std::memset(&d.tm_co, 0, sizeof d.tm_co);
+  std::memset(d.tm_cs, 0, sizeof d.tm_cs);
+  if (!uses_specialised_kernel(pl)) return DCL_OK;
+  // the specialised kernel stages, per tile, the original covariance box at
+  // (vx0 - wsh + G, vy0 - wsh + G) and the scaled covariance box at
+  // (vx0 - phm - wsh + G, vy0 - phm - wsh + G), in float4 pixels: x origins
+  // in floats are multiples of 4 (16 bytes), as the TMA unit requires
+  const FastStage fs = fast_stage(pl.P.wsh, pl.P.phm);
+  const uint64_t Hp = (uint64_t)g.Hp, pitch = (uint64_t)g.pitch;
+  int rc = encode_map_2d(&d.tm_co, d.cori, 4 * pitch, Hp, pitch * 16, 4 * fs.RO, fs.RO);
+  for (size_t si = 0; si < pl.scales.size() && rc == DCL_OK; ++si)
+    if (pl.slot_used[si]) rc = encode_map_2d(&d.tm_cs[si], d.cs[si], 4 * pitch, Hp, pitch * 16, 4 * fs.RS, fs.RS);
+  return rc;
 }
 
 // Optional timing of the fused kernel (dcl_profile_begin / dcl_profile_end):
@@ -445,7 +499,11 @@ int run_device(const Plan& pl0, const std::vector<SceneIO>& io, cudaStream_t st)
   int tb = 0;
   for (size_t i = 0; i < io.size(); ++i) {
     std::memset(&desc[i], 0, sizeof(SceneDesc));
-    carve_scene(pl, geo[i], scratch + offs[i], desc[i]);
+    rc = carve_scene(pl, geo[i], scratch + offs[i], desc[i]);
+    if (rc) {
+      cudaFreeAsync(scratch, st);
+      return rc;
+    }
     desc[i].ref = io[i].ref;
     desc[i].phase = io[i].phase;
     desc[i].coh = io[i].coh;
@@ -506,6 +564,11 @@ int run_host_insar(const Plan& pl, const float* a1, const float* a2, const float
   cudaFreeAsync(buf, st);
   cudaError_t e2 = cudaStreamSynchronize(st);
   if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR");
+  if (rc == DCL_OK && uses_specialised_kernel(pl)) {
+    int timeouts = 0;
+    if (take_stage_timeouts(&timeouts) != 0 || timeouts != 0)
+      rc = set_error(DCL_ERR_CUDA, "NL-SAR: %d tiles gave up waiting for their TMA staging copies", timeouts);
+  }
   return rc;
 }
 

@@ -97,8 +97,9 @@ __global__ void prep_scale_kernel(const float4* __restrict__ cori, int Hp, int W
   }
   const size_t o = (size_t)py * pitch + px;
   cs[o] = make_float4(c00, c11, re, im);
-  // sim_measures.h:31-34
-  const float det = (c00 * c11) - (re * re + im * im);
+  // sim_measures.h:31-34, each product and sum rounded separately (the
+  // specialised kernel recomputes it the same way from its staged copy)
+  const float det = __fsub_rn(__fmul_rn(c00, c11), __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im)));
   ld[o] = logf(det);
 }
 

@@ -97,7 +97,8 @@ extern "C" int dcl_nlsar_insar_device_noalloc(const float* a1, const float* a2, 
 
   SceneDesc d;
   std::memset(&d, 0, sizeof d);
-  carve_scene(pl, g, scratch, d);
+  rc = carve_scene(pl, g, scratch, d);
+  if (rc) return rc;
   d.ref = ref;
   d.phase = phase;
   d.coh = coh;

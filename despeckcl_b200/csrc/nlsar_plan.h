@@ -33,7 +33,7 @@ int make_plan(int sws, const int* patches, int np, const int* scales, int ns, co
 int choose_k(const Plan& pl, size_t& smem_bytes);
 SceneGeom scene_geom(const Plan& pl, int H, int W);
 size_t scratch_bytes(const Plan& pl, const SceneGeom& g);
-void carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d);
+int carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d);
 int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
                 const float* phi, const float* cov_in, cudaStream_t st);
 // variant selects the specialised kernel's instantiation (see launch_nlsar_fast)

@@ -236,7 +236,14 @@ bool dcl_server::admit_locked() {
     if (!arena.alloc(r->bytes, &off)) break;
     r->off = off;
     char* base = arena_base + off;
-    carve_scene(pl, r->g, base, r->desc);
+    const int crc = carve_scene(pl, r->g, base, r->desc);
+    if (crc != DCL_OK) {
+      // the request holds its arena block until finish_locked releases it
+      queued.pop_front();
+      finish_locked(r, crc, dcl_last_error(), now());
+      any = true;
+      continue;
+    }
     r->desc.ref = r->ref;
     r->desc.phase = r->phase;
     r->desc.coh = r->coh;
