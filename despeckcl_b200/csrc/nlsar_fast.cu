@@ -186,9 +186,8 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
     const int lt = tile - S.tile_begin + S.tile_skip;
     const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
     const int vy0 = ty * C::TH, vx0 = tx * TW;
-    const int G = P.G, pitch = S.pitch;
+    const int G = P.G;
 
-    (void)pitch;
     // stage the original covariance (tile + search halo) and the first
     // pass's scaled covariance (tile + patch and search halo) with TMA; the
     // barrier orders every thread's reads of the previous tile before the
