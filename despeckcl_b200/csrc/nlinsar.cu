@@ -43,8 +43,8 @@ namespace dcl {
 namespace {
 
 constexpr int kTile = 80;        // nlinsar.cpp:84, tile_dims {80, 80}
-constexpr int kThreads = 256;    // weights kernel
-constexpr int kMaxPixPerThread = 23;
+constexpr int kThreads = 1024;   // weights kernel (32 warps: the one CTA an SM holds)
+constexpr int kMaxPixPerThread = 6;
 constexpr int kMaxLmin = 64;
 constexpr int kEstThreads = 128;
 
