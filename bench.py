@@ -46,8 +46,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=None, help="scene side (plain: 4096, secondary: 8192)")
     p.add_argument("--mode", default="argmax_enl", choices=["argmax_enl", "reference"])
-    p.add_argument("--cpu-sample", type=int, default=704,
-                   help="side of the CPU-baseline crop (about 10 s of oracle work on 16 host cores)")
+    p.add_argument("--cpu-sample", type=int, default=1536,
+                   help="side of the CPU-baseline crop (about 10-15 s of oracle work on 16 host cores)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--config", default="plain", choices=["plain", "batched", "serving", "secondary"],
                    help="plain: one 4096x4096 scene (the headline); batched: 48 scenes of uneven size; "
