@@ -46,7 +46,7 @@ def _rank_main(rank, world, port, out):
 
 def test_two_gloo_ranks_take_the_slowest_time_and_filter_distinct_scenes():
     world, port = 2, _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
