@@ -32,10 +32,19 @@ sys.path.insert(0, ROOT)
 METRIC = "NL-SAR Mpix/s"
 UNIT = "Mpix/s"
 SWS, PATCHES, SCALES, H_PARAM, C_PARAM = 21, [3, 5, 7], [1, 3], 15.0, 49.0
-# algorithmic FP32 work per output pixel at these parameters (FMA = 2 flops):
-# pixel similarity 6160 + box sums 5280 + weights 13200 + ENL statistics
-# 29106 + selection 180 + weighted mean 3984 + per-pixel set-up/decompose 46
+# algorithmic FP32 work per output pixel at these parameters (FMA = 2 flops),
+# ENL-argmax selection (every (patch, scale) combination): pixel similarity
+# 6160 + box sums 5280 + weights 13200 + ENL statistics 29106 + statistics
+# finalisation 180 + selection 6 + weighted mean 3984 + set-up/decompose 40
 FLOP_PER_PIXEL = 57956
+# reference selection (the last statistics key only, patch 7 at scale 3):
+# similarity 3080 + box sums 880 + weights 2200 + ENL statistics 4851 +
+# finalisation 30 + selection 1 + weighted mean 3984 + set-up/decompose 40
+FLOP_PER_PIXEL_REFERENCE_MODE = 15066
+
+
+def flop_per_pixel(mode):
+    return FLOP_PER_PIXEL if mode == "argmax_enl" else FLOP_PER_PIXEL_REFERENCE_MODE
 
 
 def parse():
@@ -303,7 +312,7 @@ def run_ours(args):
     if L.dcl_measure_fp32_tflops(ctypes.byref(peak)) != 0:
         raise RuntimeError(L.dcl_last_error().decode())
     kern_ms = fused_ms.value / max(1, fused_n.value)
-    achieved = FLOP_PER_PIXEL * S * S / (kern_ms * 1e-3) / 1e12
+    achieved = flop_per_pixel(args.mode) * S * S / (kern_ms * 1e-3) / 1e12
     traffic = traffic_from_profiles(S)
 
     cpu = None
@@ -330,7 +339,7 @@ def run_ours(args):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value, "traffic": traffic,
                          "kernel": "nlsar_fast_kernel<10,1,2,3> (specialised fused NL-SAR)", "kernel_ms": kern_ms,
-                         "flop_per_pixel": FLOP_PER_PIXEL,
+                         "flop_per_pixel": flop_per_pixel(args.mode),
                          "peak_source": "measured in-process FP32 FMA probe (dcl_measure_fp32_tflops)"},
             "gpu_launches": int(all_n.value),
             "clocks": clocks,
