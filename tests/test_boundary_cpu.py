@@ -57,6 +57,26 @@ def test_argument_validation_happens_on_the_host(kw, code):
     assert e.value.code == code
 
 
+@pytest.mark.parametrize("shape", [(0, 8), (8, 0), (0, 0)])
+def test_empty_scene_is_rejected_on_the_host(shape):
+    stats = {(3, s): _stats_entry(3, s) for s in (1, 3)}
+    a = np.ones(shape, np.float32)
+    with pytest.raises(dcl.DespeckclError) as e:
+        dcl.nlsar_insar(a, a, a, 21, [3], [1, 3], stats)
+    assert e.value.code == -1
+    for fn, args in ((dcl.boxcar, (5,)), (dcl.goldstein, (32, 4, 0.5)), (dcl.nlinsar, (21, 7, 1, 10))):
+        with pytest.raises(dcl.DespeckclError) as e:
+            fn(a, a, a, *args)
+        assert e.value.code == -1
+
+
+def test_ragged_inputs_are_rejected():
+    stats = {(3, s): _stats_entry(3, s) for s in (1, 3)}
+    a, b = np.ones((8, 8), np.float32), np.ones((8, 9), np.float32)
+    with pytest.raises((dcl.DespeckclError, ValueError)):
+        dcl.nlsar_insar(a, b, a, 21, [3], [1, 3], stats)
+
+
 @pytest.mark.parametrize("dim", [1, 4])
 def test_covariance_dimension_outside_2_and_3_is_rejected(dim):
     # 2x2 and 3x3 covariances are filtered; any other size is an invalid
