@@ -63,6 +63,7 @@ def parse():
                         "serving: Poisson request streams through the request server; secondary: Goldstein, "
                         "boxcar and NL-InSAR on an 8192x8192 scene")
     p.add_argument("--nlinsar-size", type=int, default=2048, help="secondary: side of the NL-InSAR scene")
+    p.add_argument("--polsar-size", type=int, default=1024, help="secondary: side of the 3x3 covariance scene")
     p.add_argument("--requests", type=int, default=96, help="serving: requests per stream")
     p.add_argument("--hbm-budget-gb", type=float, default=120.0, help="serving: admission budget")
     return p.parse_args()
@@ -565,6 +566,8 @@ def run_secondary(args):
     (window 7) and NL-InSAR (search 21, patch 7, lmin 10; one pass per step,
     --nlinsar-size scene).  Each is timed with CUDA events on the launching
     stream over K steps with inputs resident in HBM, larger than L2."""
+    import ctypes
+
     import torch
 
     import despeckcl_b200 as dcl
@@ -620,11 +623,43 @@ def run_secondary(args):
         ms, n = timed(lambda: dcl.nlinsar_device(n1, n2, nph, 21, 7, 1, 10, estimates=est, stream=stream))
         res["nlinsar"] = {"mpix_s_per_pass": Sn * Sn / (ms * 1e-3) / 1e6, "ms_per_pass": ms, "side": Sn,
                           "launches_per_step": n / k}
+        # NL-SAR on a 3x3 (PolSAR) covariance image: single-look three-channel
+        # speckle k = L x per pixel (one random covariance), planes [18][H][W];
+        # statistics trained on a homogeneous 128 x 128 crop of it
+        Sp = min(args.polsar_size, S)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(7)
+        z = torch.randn((3, 5), generator=g, device="cuda", dtype=torch.complex64)
+        Lc = torch.linalg.cholesky(z @ z.conj().T / 5)
+        x = torch.randn((3, Sp * Sp), generator=g, device="cuda", dtype=torch.complex64)
+        kv = (Lc @ x).reshape(3, Sp, Sp)
+        cov = kv[:, None] * kv[None, :].conj()
+        planes = torch.empty((18, Sp, Sp), device="cuda")
+        planes[0::2] = cov.real.reshape(9, Sp, Sp)
+        planes[1::2] = cov.imag.reshape(9, Sp, Sp)
+        tr = planes[:, :128, :128].cpu().numpy()
+        cplx = (tr[0::2] + 1j * tr[1::2]).reshape(3, 3, 128, 128)
+        st3 = dcl.nlsar_train(cplx, PATCHES, SCALES)
+        out3 = torch.empty_like(planes)
+        import despeckcl_b200.api as api
+        pk, pp, npn = api._ints(PATCHES)
+        sk, sp, nsn = api._ints(SCALES)
+        arr, ns3, keep = api._entries(st3)
+
+        def polsar():
+            api._check(L.dcl_nlsar_covmat_device(api._dptr(planes), api._dptr(out3), Sp, Sp, 3, SWS, pp, npn, sp,
+                                                 nsn, arr, ns3, ctypes.c_float(H_PARAM), ctypes.c_float(C_PARAM),
+                                                 api._mode(args.mode), api._stream(stream)))
+
+        ms, n = timed(polsar)
+        res["nlsar_3x3"] = {"mpix_s": Sp * Sp / (ms * 1e-3) / 1e6, "ms": ms, "side": Sp, "select_mode": args.mode,
+                            "launches_per_step": n / k}
     line = {"metric": "secondary filters Mpix/s", "value": res["goldstein"]["mpix_s"], "unit": UNIT, "n_gpus": 1,
             "steps": k, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (generated on the device, seed 4)",
             "config": {"workload": f"{S}x{S} scene: Goldstein p32 ov4 a0.5, boxcar w7, NL-InSAR sws21 p7 lmin10 "
-                                   f"one pass on {min(args.nlinsar_size, S)}^2",
+                                   f"one pass on {min(args.nlinsar_size, S)}^2, NL-SAR 3x3 covariances on "
+                                   f"{min(args.polsar_size, S)}^2",
                        "l2": f"inputs {3 * S * S * 4 / 1e6:.0f} MB > L2 126 MB"},
             "hbm_peak_source": hbm_src, "filters": res, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
