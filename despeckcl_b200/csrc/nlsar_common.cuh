@@ -120,12 +120,14 @@ __host__ __device__ inline SmemLayout smem_layout(int tile_h, int wsh, int phm, 
   return L;
 }
 
+// The prep kernels fill frame rows [row0, row1) of their outputs (the grid
+// covers those rows); reads are clamped to the whole frame.
 __global__ void prep_cov_insar_kernel(const float* a1, const float* a2, const float* phi, int H, int W,
-                                      float4* cori, int Hp, int Wp, int pitch, int G);
+                                      float4* cori, int Hp, int Wp, int pitch, int G, int row0, int row1);
 __global__ void prep_cov_planes_kernel(const float* cin, int H, int W, float4* cori, float4* cori2, int Hp, int Wp,
-                                       int pitch, int G);
+                                       int pitch, int G, int row0, int row1);
 __global__ void prep_scale_kernel(const float4* cori, int Hp, int Wp, int pitch, int s, GaussArg ga, float gamma,
-                                  float4* cs, float* ld);
+                                  float4* cs, float* ld, int row0, int row1);
 // Launches the fused kernel: one CTA per tile (grid = tiles), `smem` bytes of
 // dynamic shared memory; full8 selects the 8-plane covariance variant.
 cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, int grid,

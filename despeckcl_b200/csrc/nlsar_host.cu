@@ -408,29 +408,39 @@ bool uses_specialised_kernel(const Plan& pl) {
   return !pl.full8 && !g_force_generic && fast_kernel_supported(pl.P);
 }
 
-int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
-                const float* phi, const float* cov_in, cudaStream_t st) {
-  dim3 blk(32, 8), grd((g.Wp + 31) / 32, (g.Hp + 7) / 8);
-  int used = 0;
-  for (char u : pl.slot_used) used += u ? 1 : 0;
-  profile_count(1 + used);
-  if (pl.full8)
-    prep_cov_planes_kernel<<<grd, blk, 0, st>>>(cov_in, g.H, g.W, const_cast<float4*>(d.cori),
-                                                const_cast<float4*>(d.cori2), g.Hp, g.Wp, g.pitch, pl.P.G);
-  else
-    prep_cov_insar_kernel<<<grd, blk, 0, st>>>(a1, a2, phi, g.H, g.W, const_cast<float4*>(d.cori), g.Hp, g.Wp,
-                                               g.pitch, pl.P.G);
+int launch_prep_rows(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
+                     const float* phi, const float* cov_in, int co0, int co1, int cs0, int cs1, cudaStream_t st) {
+  const dim3 blk(32, 8);
+  const unsigned gx = (unsigned)(g.Wp + 31) / 32;
+  if (co1 > co0) {
+    profile_count(1);
+    const dim3 grd(gx, (unsigned)(co1 - co0 + 7) / 8);
+    if (pl.full8)
+      prep_cov_planes_kernel<<<grd, blk, 0, st>>>(cov_in, g.H, g.W, const_cast<float4*>(d.cori),
+                                                  const_cast<float4*>(d.cori2), g.Hp, g.Wp, g.pitch, pl.P.G, co0, co1);
+    else
+      prep_cov_insar_kernel<<<grd, blk, 0, st>>>(a1, a2, phi, g.H, g.W, const_cast<float4*>(d.cori), g.Hp, g.Wp,
+                                                 g.pitch, pl.P.G, co0, co1);
+  }
+  if (cs1 <= cs0) return DCL_OK;
   const float gamma = rescale_gamma_2x2();
+  const dim3 grd(gx, (unsigned)(cs1 - cs0 + 7) / 8);
   for (size_t si = 0; si < pl.scales.size(); ++si) {
     if (!pl.slot_used[si]) continue;
     GaussArg ga;
     std::memset(&ga, 0, sizeof ga);
     const std::vector<float> gw = gauss_weights(pl.scales[si]);
     std::copy(gw.begin(), gw.end(), ga.g);
+    profile_count(1);
     prep_scale_kernel<<<grd, blk, 0, st>>>(d.cori, g.Hp, g.Wp, g.pitch, pl.scales[si], ga, gamma,
-                                           const_cast<float4*>(d.cs[si]), const_cast<float*>(d.ld[si]));
+                                           const_cast<float4*>(d.cs[si]), const_cast<float*>(d.ld[si]), cs0, cs1);
   }
   return DCL_OK;
+}
+
+int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
+                const float* phi, const float* cov_in, cudaStream_t st) {
+  return launch_prep_rows(pl, g, d, a1, a2, phi, cov_in, 0, g.Hp, 0, g.Hp, st);
 }
 
 int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st,
@@ -532,37 +542,161 @@ int run_device(const Plan& pl0, const std::vector<SceneIO>& io, cudaStream_t st)
   return DCL_OK;
 }
 
-// host pointers: copy in, run, copy out (the reference's filter_sub_image
-// uploads and downloads the same way, nlsar/conversion.cpp:22-142)
-int run_host_insar(const Plan& pl, const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+// Copy streams and events of the calling thread's host-pointer calls, one
+// set per device, created on first use and kept for the thread's lifetime.
+struct HostPipe {
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> ev;
+};
+static thread_local HostPipe g_pipes[kMaxDevices];
+
+static int host_pipe(int dev, size_t nev, HostPipe*& out) {
+  if (dev < 0 || dev >= kMaxDevices) return set_error(DCL_ERR_CUDA, "device %d out of range", dev);
+  HostPipe& p = g_pipes[dev];
+  cudaError_t e = cudaSuccess;
+  if (!p.h2d) e = cudaStreamCreateWithFlags(&p.h2d, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !p.d2h) e = cudaStreamCreateWithFlags(&p.d2h, cudaStreamNonBlocking);
+  while (e == cudaSuccess && p.ev.size() < nev) {
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) p.ev.push_back(ev);
+  }
+  if (e != cudaSuccess) return cuda_error(e, "host copy streams");
+  out = &p;
+  return DCL_OK;
+}
+
+constexpr int kMaxBands = 8;      // row bands of a host-pointer call
+constexpr int kBandTileRows = 8;  // fewest tile rows per band
+
+// Host pointers: the reference's filter_sub_image uploads the inputs and
+// downloads the results around its kernels (nlsar/conversion.cpp:22-142).
+// Here the scene is cut into bands of tile rows and the copies overlap the
+// filtering: band b's input rows go up on their own stream while band b-1 is
+// filtered, and every band's results come down on a third stream as soon as
+// its tiles are done.  The frames are filled band by band (each prep kernel
+// only on rows whose inputs have arrived), so every tile reads exactly the
+// values of the single-launch path and the results are identical.
+// The downloads are issued after all bands are queued, so a pageable
+// destination (a synchronous copy) still lets the later bands run meanwhile.
+int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const float* phi, float* ref, float* phase,
                    float* coh, int H, int W) {
   if (!a1 || !a2 || !phi || !ref || !phase || !coh) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
   int dev;
   int rc = ensure_device_ready(dev);
   if (rc) return rc;
+  Plan pl = pl0;
+  size_t smem = 0;
+  const int K = choose_k(pl, smem);
+  if (K < 1) return set_error(DCL_ERR_UNSUPPORTED, "search window / patch sizes too large for shared memory");
+  pl.P.K = K;
+  const SceneGeom g = scene_geom(pl, H, W);
+  if ((long long)g.tiles_x * g.tiles_y > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
+  const int nb = std::max(1, std::min(kMaxBands, g.tiles_y / kBandTileRows));
+  HostPipe* hp = nullptr;
+  rc = host_pipe(dev, 2 * (size_t)nb + 2, hp);
+  if (rc) return rc;
+  cudaEvent_t* ev_in = hp->ev.data();       // band inputs uploaded
+  cudaEvent_t* ev_out = hp->ev.data() + nb;  // band results written
+  cudaEvent_t ev_alloc = hp->ev[2 * nb], ev_done = hp->ev[2 * nb + 1];
+
   cudaStream_t st = cudaStreamPerThread;
   const size_t n = (size_t)H * W, b = n * sizeof(float);
-  float* buf = nullptr;
-  cudaError_t e = cudaMallocAsync(&buf, 6 * b, st);
-  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io)");
-  e = cudaMemcpyAsync(buf, a1, b, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n, a2, b, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 2 * n, phi, b, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    cudaFreeAsync(buf, st);
-    return cuda_error(e, "cudaMemcpyAsync(H2D)");
+  const size_t scratch = (scratch_bytes(pl, g) + 255) / 256 * 256;
+  const size_t desc_bytes = (nb * sizeof(SceneDesc) + 255) / 256 * 256;
+  const size_t wtab_bytes = pl.wtab.size() * sizeof(float);
+  const size_t io_bytes = (6 * b + 255) / 256 * 256;
+  char* mem = nullptr;
+  cudaError_t e = cudaMallocAsync(&mem, io_bytes + scratch + desc_bytes + wtab_bytes, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io + scratch)");
+  float* buf = reinterpret_cast<float*>(mem);
+  SceneDesc* d_desc = reinterpret_cast<SceneDesc*>(mem + io_bytes + scratch);
+  float* d_wtab = reinterpret_cast<float*>(mem + io_bytes + scratch + desc_bytes);
+
+  // band b covers tile rows [tb[b], tb[b+1])
+  std::vector<int> tb(nb + 1);
+  for (int i = 0; i <= nb; ++i) tb[i] = (int)((long long)g.tiles_y * i / nb);
+  std::vector<SceneDesc> desc(nb);
+  std::memset(desc.data(), 0, nb * sizeof(SceneDesc));
+  rc = carve_scene(pl, g, mem + io_bytes, desc[0]);
+  for (int i = 0; i < nb && rc == DCL_OK; ++i) {
+    if (i) desc[i] = desc[0];
+    desc[i].ref = buf + 3 * n;
+    desc[i].phase = buf + 4 * n;
+    desc[i].coh = buf + 5 * n;
+    desc[i].tile_begin = 0;
+    desc[i].tile_skip = tb[i] * g.tiles_x;
   }
-  SceneIO s{buf, buf + n, buf + 2 * n, nullptr, buf + 3 * n, buf + 4 * n, buf + 5 * n, nullptr, nullptr, H, W};
-  rc = run_device(pl, {s}, st);
   if (rc == DCL_OK) {
-    e = cudaMemcpyAsync(ref, buf + 3 * n, b, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(phase, buf + 4 * n, b, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(coh, buf + 5 * n, b, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(d_desc, desc.data(), nb * sizeof(SceneDesc), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_wtab, pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_alloc, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp->h2d, ev_alloc, 0);
+    if (e != cudaSuccess) rc = cuda_error(e, "NL-SAR parameters");
+  }
+  pl.P.wtab = d_wtab;
+  pl.P.n_scenes = 1;
+
+  const int TH = pl.P.tile_h, G = pl.P.G;
+  int in_done = 0, co_done = 0, cs_done = 0;
+  for (int i = 0; i < nb && rc == DCL_OK; ++i) {
+    const bool last = i == nb - 1;
+    // frame rows the band's tiles read (scaled covariance: tile + patch and
+    // search halo), the original-covariance rows those average over, and the
+    // input rows behind them (frame row r holds input row r - G, clamped)
+    const int cs_need = last ? g.Hp : std::min(g.Hp, tb[i + 1] * TH + pl.P.phm + pl.P.wsh + G);
+    const int co_need = last ? g.Hp : std::min(g.Hp, cs_need + pl.shm);
+    const int in_need = last ? H : std::max(1, std::min(H, co_need - G));
+    if (in_need > in_done) {
+      const size_t off = (size_t)in_done * W, cnt = (size_t)(in_need - in_done) * W * sizeof(float);
+      e = cudaMemcpyAsync(buf + off, a1 + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n + off, a2 + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 2 * n + off, phi + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
+      in_done = in_need;
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev_in[i], hp->h2d);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev_in[i], 0);
+    if (e != cudaSuccess) {
+      rc = cuda_error(e, "cudaMemcpyAsync(H2D)");
+      break;
+    }
+    launch_prep_rows(pl, g, desc[i], buf, buf + n, buf + 2 * n, nullptr, co_done, co_need, cs_done, cs_need, st);
+    co_done = co_need;
+    cs_done = cs_need;
+    FilterParams F = pl.P;
+    F.total_tiles = (tb[i + 1] - tb[i]) * g.tiles_x;
+    if (F.total_tiles > 0) rc = launch_fused(pl, F, d_desc + i, smem, st);
+    e = cudaGetLastError();
+    if (rc == DCL_OK && e != cudaSuccess) rc = cuda_error(e, "NL-SAR launch");
+    if (rc == DCL_OK && (e = cudaEventRecord(ev_out[i], st)) != cudaSuccess) rc = cuda_error(e, "event");
+  }
+  // results: band b holds output rows [tb[b] * TH, tb[b+1] * TH) below row
+  // H-1; row H-1 comes from the last tile row (virtual row H-1+overlap)
+  for (int i = 0; i < nb && rc == DCL_OK; ++i) {
+    const int r0 = std::min(tb[i] * TH, H - 1);
+    const int r1 = i == nb - 1 ? H : std::min(tb[i + 1] * TH, H - 1);
+    e = cudaStreamWaitEvent(hp->d2h, ev_out[i], 0);
+    if (r1 > r0) {
+      const size_t off = (size_t)r0 * W, cnt = (size_t)(r1 - r0) * W * sizeof(float);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ref + off, buf + 3 * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(phase + off, buf + 4 * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(coh + off, buf + 5 * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
+    }
     if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
   }
-  cudaFreeAsync(buf, st);
-  cudaError_t e2 = cudaStreamSynchronize(st);
+  // the buffers are freed in stream order after every copy that uses them
+  cudaError_t e2 = cudaEventRecord(ev_done, hp->d2h);
+  if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(st, ev_done, 0);
+  cudaError_t e3 = cudaEventRecord(ev_done, hp->h2d);
+  if (e3 == cudaSuccess) e3 = cudaStreamWaitEvent(st, ev_done, 0);
+  if (e2 != cudaSuccess || e3 != cudaSuccess) {
+    // ordering could not be expressed: wait for the copy streams on the host
+    cudaStreamSynchronize(hp->h2d);
+    cudaStreamSynchronize(hp->d2h);
+  }
+  cudaFreeAsync(mem, st);
+  e2 = cudaStreamSynchronize(st);
   if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR");
   if (rc == DCL_OK && uses_specialised_kernel(pl)) {
     int timeouts = 0;

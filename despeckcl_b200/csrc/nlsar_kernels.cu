@@ -47,10 +47,10 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // (covmat_create.cl:32-42; clamp padding as src/data/sub_images.cpp:37-38).
 __global__ void prep_cov_insar_kernel(const float* __restrict__ a1, const float* __restrict__ a2,
                                       const float* __restrict__ phi, int H, int W, float4* __restrict__ cori,
-                                      int Hp, int Wp, int pitch, int G) {
+                                      int Hp, int Wp, int pitch, int G, int row0, int row1) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
-  const int py = blockIdx.y * blockDim.y + threadIdx.y;
-  if (px >= Wp || py >= Hp) return;
+  const int py = row0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= row1) return;
   const int y = clampi(py - G, 0, H - 1), x = clampi(px - G, 0, W - 1);
   const size_t i = (size_t)y * W + x;
   const float am = a1[i], as = a2[i];
@@ -62,10 +62,11 @@ __global__ void prep_cov_insar_kernel(const float* __restrict__ a1, const float*
 
 // Un-rescaled covariance from an 8-plane covariance image.
 __global__ void prep_cov_planes_kernel(const float* __restrict__ cin, int H, int W, float4* __restrict__ cori,
-                                       float4* __restrict__ cori2, int Hp, int Wp, int pitch, int G) {
+                                       float4* __restrict__ cori2, int Hp, int Wp, int pitch, int G, int row0,
+                                       int row1) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
-  const int py = blockIdx.y * blockDim.y + threadIdx.y;
-  if (px >= Wp || py >= Hp) return;
+  const int py = row0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= row1) return;
   const int y = clampi(py - G, 0, H - 1), x = clampi(px - G, 0, W - 1);
   const size_t n = (size_t)H * W, i = (size_t)y * W + x;
   cori[(size_t)py * pitch + px] = make_float4(cin[i], cin[6 * n + i], cin[2 * n + i], cin[3 * n + i]);
@@ -77,10 +78,10 @@ __global__ void prep_cov_planes_kernel(const float* __restrict__ cin, int H, int
 // averaged (covmat_spatial_avg.cl:50-57, weights of
 // cl_wrappers/covmat_spatial_avg.cpp:35-50) covariance of one scale, plus ln det.
 __global__ void prep_scale_kernel(const float4* __restrict__ cori, int Hp, int Wp, int pitch, int s, GaussArg ga,
-                                  float gamma, float4* __restrict__ cs, float* __restrict__ ld) {
+                                  float gamma, float4* __restrict__ cs, float* __restrict__ ld, int row0, int row1) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
-  const int py = blockIdx.y * blockDim.y + threadIdx.y;
-  if (px >= Wp || py >= Hp) return;
+  const int py = row0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= row1) return;
   const int ssh = (s - 1) / 2;
   float c00 = 0.f, c11 = 0.f, re = 0.f, im = 0.f;
   for (int kx = 0; kx < s; ++kx) {

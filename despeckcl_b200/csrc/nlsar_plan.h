@@ -36,6 +36,10 @@ size_t scratch_bytes(const Plan& pl, const SceneGeom& g);
 int carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d);
 int launch_prep(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
                 const float* phi, const float* cov_in, cudaStream_t st);
+// the same for frame rows [co0, co1) of the original covariance and [cs0, cs1)
+// of every scaled covariance (the rows those read must be filled already)
+int launch_prep_rows(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
+                     const float* phi, const float* cov_in, int co0, int co1, int cs0, int cs1, cudaStream_t st);
 // variant selects the specialised kernel's instantiation (see launch_nlsar_fast)
 int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, cudaStream_t st,
                  int variant = 0);

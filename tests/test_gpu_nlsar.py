@@ -221,6 +221,18 @@ def test_host_entry_point_equals_device_entry_point(train_stats):
         np.testing.assert_array_equal(h, d)
 
 
+@pytest.mark.parametrize("shape,mode", [((1061, 97), "argmax_enl"), ((520, 64), "reference"),
+                                        ((777, 41), "argmax_enl")])
+def test_banded_host_entry_point_equals_device_entry_point(train_stats, shape, mode):
+    # scenes of 16+ tile rows go through the host entry point in row bands
+    # whose copies overlap the filtering; results must equal one launch's
+    a1, a2, ph = synthetic.insar_scene(*shape, 21)
+    host = dcl.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=mode)
+    dev = run_gpu(a1, a2, ph, train_stats, mode)
+    for h, d in zip(host, dev):
+        np.testing.assert_array_equal(h, d)
+
+
 def test_shift_invariance_is_bit_exact(train_stats):
     # each output pixel depends only on its overlap-radius neighbourhood, so a
     # crop filtered alone reproduces the interior of the full scene exactly
