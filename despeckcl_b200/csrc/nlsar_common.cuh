@@ -43,6 +43,7 @@ struct SceneDesc {
   // [Hp][4 pitch] of the cori and cs[s] frames with the boxes of one tile's
   // staged regions; zero when that kernel is not used
   CUtensorMap tm_co;
+  CUtensorMap tm_co2;  // cori2 (8-plane covariance input)
   CUtensorMap tm_cs[kMaxScales];
   const float4* cori;   // un-rescaled covariance {C00, C11, Re C01, Im C01}
   const float4* cori2;  // covariance path only: {Im C00, Re C10, Im C10, Im C11}
@@ -133,15 +134,22 @@ __global__ void prep_scale_kernel(const float4* cori, int Hp, int Wp, int pitch,
 cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, int grid,
                                cudaStream_t st);
 
-// Staged regions of the specialised kernel's tile (32 x 32 outputs), in
-// pixels: scaled covariance RS x RS, original covariance RO x RO.
+// Tile rows of the specialised kernel: InSAR input, 8-plane covariance input.
+constexpr int kFastTileH = 32;
+constexpr int kFastTileH8 = 24;
+
+// Staged regions of the specialised kernel's tile (32 x tile_h outputs), in
+// pixels (width x height): scaled covariance RS x RSH, original covariance
+// RO x ROH.
 struct FastStage {
-  int RS, RO;
+  int RS, RSH, RO, ROH;
 };
-__host__ __device__ inline FastStage fast_stage(int wsh, int phm) {
+__host__ __device__ inline FastStage fast_stage(int wsh, int phm, int tile_h) {
   FastStage f;
   f.RS = 32 + 2 * (phm + wsh);
+  f.RSH = tile_h + 2 * (phm + wsh);
   f.RO = 32 + 2 * wsh;
+  f.ROH = tile_h + 2 * wsh;
   return f;
 }
 
@@ -152,6 +160,6 @@ bool fast_kernel_supported(const FilterParams& F);
 // since the last call (the count is reset); 0 on success, -1 on a CUDA error
 int take_stage_timeouts(int* count);
 cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
-                              int variant = 0);
+                              int variant = 0, bool full8 = false);
 
 }  // namespace dcl

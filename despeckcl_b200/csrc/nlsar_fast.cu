@@ -37,44 +37,53 @@ namespace {
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-template <int WSH, int PH0, int PH1, int PH2, int PX_>
+template <int WSH, int PH0, int PH1, int PH2, int PX_, int TH_, bool FULL8_>
 struct Fast {
   static constexpr int NP = (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
   static constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
   static constexpr int SWS = 2 * WSH + 1;
-  static constexpr int TH = 32, TW = 32, PX = PX_;  // vertically adjacent pixels per thread (2 or 4)
+  static constexpr bool FULL8 = FULL8_;              // 8-plane covariance input and output
+  static constexpr int TH = TH_, TW = 32, PX = PX_;  // tile rows; vertically adjacent pixels per thread
   static constexpr int WARPS = TH / PX, THREADS = 32 * WARPS;
-  static constexpr int K = 3;                       // offsets per batch (SWS % K == 0)
-  static constexpr int RS = TW + 2 * (PHM + WSH);   // scaled covariance region (square)
-  static constexpr int RO = TW + 2 * WSH;           // original covariance region
-  static constexpr int SIMW = TW + 2 * PHM;         // similarity region (square)
+  static constexpr int K = 3;                        // offsets per batch (SWS % K == 0)
+  static constexpr int NA = FULL8 ? 12 : 8;          // accumulators per (pixel, patch size)
+  static constexpr int NM = FULL8 ? 8 : 4;           // weighted sums kept for the selected combination
+  static constexpr int RS = TW + 2 * (PHM + WSH);    // scaled covariance region: RS x RSH
+  static constexpr int RSH = TH + 2 * (PHM + WSH);
+  static constexpr int RO = TW + 2 * WSH;            // original covariance region: RO x ROH
+  static constexpr int ROH = TH + 2 * WSH;
+  static constexpr int SIMW = TW + 2 * PHM;          // similarity region: SIMW x SIMH
+  static constexpr int SIMH = TH + 2 * PHM;
   // similarity row pitch, a multiple of 8 words: phase A's lanes write
   // consecutive words; phase B reads 16-byte vectors, a quarter warp covering
   // 8 consecutive segments of one row (contiguous, conflict free)
   static constexpr int SIMP = (SIMW + 7) / 8 * 8;
   static constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
   static constexpr int HP = TW;                     // horizontal-sum row pitch (words), unpadded
-  static constexpr int HPL = K * SIMW * HP;         // one patch size's horizontal-sum plane
+  static constexpr int HPL = K * SIMH * HP;         // one patch size's horizontal-sum plane
   static constexpr int LUTREP = 16;                 // interleaved LUT copies: two lanes per copy
   // shared memory, in 4-byte words
   // the two TMA destinations start on 128-byte boundaries
+  // the TMA destinations start on 128-byte boundaries
   static constexpr int OFF_CS = 0;
-  static constexpr int OFF_CO = (OFF_CS + 4 * RS * RS + 31) / 32 * 32;
-  static constexpr int OFF_H = OFF_CO + 4 * RO * RO;
+  static constexpr int OFF_CO = (OFF_CS + 4 * RS * RSH + 31) / 32 * 32;
+  static constexpr int OFF_CO2 = (OFF_CO + 4 * RO * ROH + 31) / 32 * 32;  // 8-plane input only
+  static constexpr int OFF_H = OFF_CO2 + (FULL8 ? 4 * RO * ROH : 0);
   static constexpr int OFF_LD = OFF_H + NP * HPL;
-  static constexpr int OFF_SIM = OFF_LD + RS * RS;
-  static constexpr int OFF_LUT = OFF_SIM + K * SIMW * SIMP;
+  static constexpr int OFF_SIM = OFF_LD + RS * RSH;
+  static constexpr int OFF_LUT = OFF_SIM + K * SIMH * SIMP;
   static constexpr int OFF_BAR = (OFF_LUT + NP * kMaxLut * LUTREP + 1) / 2 * 2;  // the mbarrier (8 bytes)
   static constexpr int WORDS = OFF_BAR + 2;
-  static constexpr uint32_t CO_BYTES = 16u * RO * RO;  // one TMA box each
-  static constexpr uint32_t CS_BYTES = 16u * RS * RS;
+  static constexpr uint32_t CO_BYTES = 16u * RO * ROH;  // one TMA box each
+  static constexpr uint32_t CS_BYTES = 16u * RS * RSH;
   static_assert(SWS % K == 0, "offset batches must tile a window row");
   static_assert(PH0 >= 0, "at least one patch");
   static_assert(PX % 2 == 0, "pixels are accumulated in pairs");
   static_assert(SIMP % 8 == 0 && SIMP >= 4 * 7 + 4 * NQ4, "phase-B segments must stay inside a row");
   static_assert(HP >= TW && HP % 4 == 0, "horizontal-sum pitch");
   static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
-  static_assert(4 * RS <= 256 && 4 * RO <= 256, "TMA box sides are at most 256 elements");
+  static_assert(4 * RS <= 256 && 4 * RO <= 256 && RSH <= 256, "TMA box sides are at most 256 elements");
+  static_assert(TH % PX == 0 && TH % 4 == 0, "tile rows");
 };
 
 // ---- TMA staging through one mbarrier --------------------------------------
@@ -153,19 +162,21 @@ __device__ __forceinline__ constexpr int ph_of(int j) {
   return j == 0 ? PH0 : (j == 1 ? PH1 : PH2);
 }
 
-template <int WSH, int PH0, int PH1, int PH2, int PX_>
-__global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
+template <int WSH, int PH0, int PH1, int PH2, int PX_, int TH_, bool FULL8_>
+__global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
-  using C = Fast<WSH, PH0, PH1, PH2, PX_>;
-  constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RO = C::RO;
-  constexpr int SIMW = C::SIMW, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
-  constexpr int NT = C::THREADS, NW = C::WARPS;
+  using C = Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>;
+  constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RSH = C::RSH, RO = C::RO;
+  constexpr int SIMW = C::SIMW, SIMH = C::SIMH, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
+  constexpr int NT = C::THREADS, NW = C::WARPS, NA = C::NA, NM = C::NM;
+  constexpr bool FULL8 = C::FULL8;
   extern __shared__ __align__(128) float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::OFF_BAR);
   float4* sCs = reinterpret_cast<float4*>(smem + C::OFF_CS);
   float4* sCo = reinterpret_cast<float4*>(smem + C::OFF_CO);
-  float* sH = smem + C::OFF_H;  // [NP][K][SIMW][HP]
+  float4* sCo2 = reinterpret_cast<float4*>(smem + C::OFF_CO2);  // 8-plane input only
+  float* sH = smem + C::OFF_H;  // [NP][K][SIMH][HP]
   float* sLd = smem + C::OFF_LD;
   float* sSim = smem + C::OFF_SIM;
   float* sLut = smem + C::OFF_LUT;
@@ -188,23 +199,24 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
     const int vy0 = ty * C::TH, vx0 = tx * TW;
     const int G = P.G;
 
-    // stage the original covariance (tile + search halo) and the first
-    // pass's scaled covariance (tile + patch and search halo) with TMA; the
-    // barrier orders every thread's reads of the previous tile before the
-    // copies overwrite shared memory
+    // stage the original covariance (tile + search halo; both of its float4
+    // planes for 8-plane input) and the first pass's scaled covariance (tile
+    // + patch and search halo) with TMA; the barrier orders every thread's
+    // reads of the previous tile before the copies overwrite shared memory
     __syncthreads();
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(bar, C::CO_BYTES + C::CS_BYTES);
+      mbar_expect_tx(bar, (FULL8 ? 2 : 1) * C::CO_BYTES + C::CS_BYTES);
       tma_load_2d(sCo, &S.tm_co, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
+      if (FULL8) tma_load_2d(sCo2, &S.tm_co2, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
       tma_load_2d(sCs, &S.tm_cs[P.pass[0].scale_slot], 4 * (vx0 - PHM - WSH + G), vy0 - PHM - WSH + G, bar);
     }
     if (!stage_wait(bar, parity)) return;
     parity ^= 1u;
-    for (int i = tid; i < RS * RS; i += NT) sLd[i] = ln_det(sCs[i]);
+    for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
 
-    float2 acc[PX / 2][NP][8];  // .x: pixel 2i, .y: pixel 2i+1
-    float best_e[PX], best_a[PX], best_s0[PX], best_m[PX][4];
+    float2 acc[PX / 2][NP][NA];  // .x: pixel 2i, .y: pixel 2i+1
+    float best_e[PX], best_a[PX], best_s0[PX], best_m[PX][NM];
     int best_rank[PX], best_combo[PX];
 #pragma unroll
     for (int i = 0; i < PX; ++i) {
@@ -214,7 +226,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       best_a[i] = 0.f;
       best_s0[i] = 1.f;
 #pragma unroll
-      for (int d = 0; d < 4; ++d) best_m[i][d] = 0.f;
+      for (int d = 0; d < NM; ++d) best_m[i][d] = 0.f;
     }
 
     int loaded_slot = P.pass[0].scale_slot;
@@ -229,7 +241,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
         }
         if (!stage_wait(bar, parity)) return;
         parity ^= 1u;
-        for (int i = tid; i < RS * RS; i += NT) sLd[i] = ln_det(sCs[i]);
+        for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
         loaded_slot = pp.scale_slot;
       }
       // composite weight tables, LUTREP interleaved copies
@@ -256,7 +268,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
 #pragma unroll
         for (int j = 0; j < NP; ++j)
 #pragma unroll
-          for (int a = 0; a < 8; ++a) acc[i][j][a] = make_float2(0.f, 0.f);
+          for (int a = 0; a < NA; ++a) acc[i][j][a] = make_float2(0.f, 0.f);
       __syncthreads();
 
       for (int dy = -WSH; dy <= WSH; ++dy) {
@@ -264,7 +276,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
           // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
           // thread and consecutive pixels on consecutive lanes (conflict free)
           // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-          for (int it = tid; it < SIMW * SIMP; it += NT) {
+          for (int it = tid; it < SIMH * SIMP; it += NT) {
             const int r = it / SIMP;
             const int c = it - r * SIMP;
             if (c >= SIMW) continue;
@@ -273,21 +285,21 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
             const float la = sLd[ci];
             const int ni = ci + dy * RS + dx0;
 #pragma unroll
-            for (int k = 0; k < K; ++k) sSim[k * SIMW * SIMP + it] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
+            for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
           }
           __syncthreads();
           // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
           // quad of rows x 8 column segments, each quarter warp one row, so its
           // 16-byte loads and stores are contiguous.
           {
-            constexpr int QUADS = (SIMW + 3) / 4;
+            constexpr int QUADS = (SIMH + 3) / 4;
             const int r_off = lane >> 3;
             const int seg = lane & 7;
             for (int q = warp; q < K * QUADS; q += NW) {
               const int k = q / QUADS;
               const int r = (q - k * QUADS) * 4 + r_off;
-              if (r < SIMW) {
-                const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMW + r) * SIMP + 4 * seg);
+              if (r < SIMH) {
+                const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
                 float s[4 * C::NQ4];
 #pragma unroll
                 for (int q4 = 0; q4 < C::NQ4; ++q4) {
@@ -317,7 +329,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
                 }
 #pragma unroll
                 for (int j = 0; j < NP; ++j)
-                  *reinterpret_cast<float4*>(sH + j * C::HPL + (k * SIMW + r) * C::HP + 4 * seg) =
+                  *reinterpret_cast<float4*>(sH + j * C::HPL + (k * SIMH + r) * C::HP + 4 * seg) =
                       make_float4(hs[j][0], hs[j][1], hs[j][2], hs[j][3]);
               }
             }
@@ -332,7 +344,7 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
             float hv[NP][PX + 2 * PHM];
 #pragma unroll
             for (int j = 0; j < NP; ++j) {
-              const float* col = sH + j * C::HPL + (k * SIMW + y0 + PHM - ph_of<PH0, PH1, PH2>(j)) * C::HP + lane;
+              const float* col = sH + j * C::HPL + (k * SIMH + y0 + PHM - ph_of<PH0, PH1, PH2>(j)) * C::HP + lane;
 #pragma unroll
               for (int r = 0; r < PX + 2 * ph_of<PH0, PH1, PH2>(j); ++r) hv[j][r] = col[r * C::HP];
             }
@@ -351,8 +363,6 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
                   float d = hv[j][i];
 #pragma unroll
                   for (int a = 1; a <= 2 * ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + a];
-                  // (unsigned)((clamp(d)-dmin)/(dmax-dmin)*(L-1)) by a saturating
-                  // FMA and a round-toward-zero add; d > dmax has weight 0
                   // index = (unsigned)((clamp(d) - dmin) / (dmax - dmin) * (L - 1)):
                   // a saturating FMA clamps (and maps NaN to 0), a round-toward-zero
                   // add of 2^23 truncates, and the float's low mantissa bits are the
@@ -369,11 +379,21 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
             // rounded exactly like the scalar add / multiply / fma
 #pragma unroll
             for (int i = 0; i < PX; i += 2) {
-              const float4 va = sCo[(y0 + i + WSH + dy) * RO + (lane + WSH + dx)];
-              const float4 vb = sCo[(y0 + i + 1 + WSH + dy) * RO + (lane + WSH + dx)];
+              const int oa = (y0 + i + WSH + dy) * RO + (lane + WSH + dx);
+              const float4 va = sCo[oa];
+              const float4 vb = sCo[oa + RO];
               const float2 vx = make_float2(va.x, vb.x), vy = make_float2(va.y, vb.y);
               const float2 vz = make_float2(va.z, vb.z), vw = make_float2(va.w, vb.w);
               const float2 x2 = __fmul2_rn(vx, vx), y2 = __fmul2_rn(vy, vy);
+              float2 ex[4];
+              if (FULL8) {
+                const float4 ea = sCo2[oa];
+                const float4 eb = sCo2[oa + RO];
+                ex[0] = make_float2(ea.x, eb.x);
+                ex[1] = make_float2(ea.y, eb.y);
+                ex[2] = make_float2(ea.z, eb.z);
+                ex[3] = make_float2(ea.w, eb.w);
+              }
 #pragma unroll
               for (int j = 0; j < NP; ++j) {
                 float2* A = acc[i / 2][j];
@@ -386,6 +406,10 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
                 A[5] = __ffma2_rn(ww, y2, A[5]);
                 A[6] = __ffma2_rn(ww, vz, A[6]);
                 A[7] = __ffma2_rn(ww, vw, A[7]);
+                if (FULL8) {
+#pragma unroll
+                  for (int e = 0; e < 4; ++e) A[(8 + e) % NA] = __ffma2_rn(ww, ex[e], A[(8 + e) % NA]);
+                }
               }
             }
           }
@@ -401,9 +425,9 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       for (int i = 0; i < PX; ++i) {
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-          float A[8];
+          float A[NA];
 #pragma unroll
-          for (int a = 0; a < 8; ++a) A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
+          for (int a = 0; a < NA; ++a) A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
           const float s0 = A[0], s1 = A[1], s2 = A[2], s3 = A[3], s4 = A[4], s5 = A[5], s6 = A[6], s7 = A[7];
           const float enl = s0 * s0 / s1;
           const float i0 = s2 / s0, i1 = s3 / s0;
@@ -430,12 +454,15 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
             best_m[i][1] = s3;
             best_m[i][2] = s6;
             best_m[i][3] = s7;
+#pragma unroll
+            for (int e = 4; e < NM; ++e) best_m[i][e] = A[(e + 4) % NA];
           }
         }
       }
     }
 
-    // ---- blend with the centre, decompose, store
+    // ---- blend with the centre (weighted_means.cl:79); InSAR input:
+    // decompose (covmat_decompose.cl:32-37), 8-plane input: the 8 planes
 #pragma unroll
     for (int i = 0; i < PX; ++i) {
       const int y = y0 + i;
@@ -443,7 +470,8 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       const int oy = (vy < S.H - 1) ? vy : (vy == S.vH ? S.H - 1 : -1);
       const int ox = (vx < S.W - 1) ? vx : (vx == S.vW ? S.W - 1 : -1);
       if (oy < 0 || ox < 0) continue;
-      const float4 c = sCo[(y + WSH) * RO + (lane + WSH)];
+      const int ci = (y + WSH) * RO + (lane + WSH);
+      const float4 c = sCo[ci];
       const float alpha = best_a[i], s0 = best_s0[i];
       const float oma = 1.0f - alpha;
       const float c00 = oma * best_m[i][0] / s0 + alpha * c.x;
@@ -451,35 +479,51 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_>::THREADS, 1)
       const float cre = oma * best_m[i][2] / s0 + alpha * c.z;
       const float cim = oma * best_m[i][3] / s0 + alpha * c.w;
       const size_t o = (size_t)oy * S.W + ox;
-      const float am = sqrtf(c00), as = sqrtf(c11);
-      const float r = 0.5f * (am + as);
-      S.ref[o] = r * r;
-      S.phase[o] = atan2f(cim, cre);
-      S.coh[o] = sqrtf(cim * cim + cre * cre) / (am * as);
+      if (FULL8) {
+        // planes {Re, Im} of C00, C01, C10, C11; the second staged float4 is
+        // {Im C00, Re C10, Im C10, Im C11}
+        const float4 c2 = sCo2[ci];
+        const size_t n = (size_t)S.H * S.W;
+        S.cov_out[o] = c00;
+        S.cov_out[n + o] = oma * best_m[i][4 % NM] / s0 + alpha * c2.x;
+        S.cov_out[2 * n + o] = cre;
+        S.cov_out[3 * n + o] = cim;
+        S.cov_out[4 * n + o] = oma * best_m[i][5 % NM] / s0 + alpha * c2.y;
+        S.cov_out[5 * n + o] = oma * best_m[i][6 % NM] / s0 + alpha * c2.z;
+        S.cov_out[6 * n + o] = c11;
+        S.cov_out[7 * n + o] = oma * best_m[i][7 % NM] / s0 + alpha * c2.w;
+      } else {
+        const float am = sqrtf(c00), as = sqrtf(c11);
+        const float r = 0.5f * (am + as);
+        S.ref[o] = r * r;
+        S.phase[o] = atan2f(cim, cre);
+        S.coh[o] = sqrtf(cim * cim + cre * cre) / (am * as);
+      }
       if (S.sel_out) S.sel_out[o] = best_combo[i];
     }
   }
 }
 
-template <int WSH, int PH0, int PH1, int PH2, int PX_>
+template <int WSH, int PH0, int PH1, int PH2, int PX_, int TH_, bool FULL8_>
 cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
-  using C = Fast<WSH, PH0, PH1, PH2, PX_>;
+  using C = Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>;
   const size_t smem = (size_t)C::WORDS * 4;
   static size_t allowed[kMaxDevices];
-  const cudaError_t e = allow_dynamic_smem((const void*)nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_>, smem, allowed);
+  const cudaError_t e =
+      allow_dynamic_smem((const void*)nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>, smem, allowed);
   if (e != cudaSuccess) return e;
-  nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
+  nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
   return cudaGetLastError();
 }
 
-template <int PX_>
+template <int PX_, int TH_, bool FULL8_>
 cudaError_t launch_fast_px(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
   const PassParams& p0 = F.pass[0];
-  if (p0.np == 3) return launch_fast_t<10, 1, 2, 3, PX_>(F, d_scenes, grid, st);
+  if (p0.np == 3) return launch_fast_t<10, 1, 2, 3, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
   switch (p0.ph[0]) {
-    case 1: return launch_fast_t<10, 1, -1, -1, PX_>(F, d_scenes, grid, st);
-    case 2: return launch_fast_t<10, 2, -1, -1, PX_>(F, d_scenes, grid, st);
-    default: return launch_fast_t<10, 3, -1, -1, PX_>(F, d_scenes, grid, st);
+    case 1: return launch_fast_t<10, 1, -1, -1, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
+    case 2: return launch_fast_t<10, 2, -1, -1, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
+    default: return launch_fast_t<10, 3, -1, -1, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
   }
 }
 
@@ -515,12 +559,16 @@ bool fast_kernel_supported(const FilterParams& F) {
   return false;
 }
 
-// variant 0: 2 pixels per thread, 512-thread CTAs (the default); variant 1:
-// 4 pixels per thread, 256-thread CTAs.  The batch autotuner times both.
+// InSAR input (32 x 32 tiles): variant 0 has 2 pixels per thread in
+// 512-thread CTAs (the default), variant 1 4 pixels per thread in 256-thread
+// CTAs; the batch autotuner times both.  8-plane covariance input: 32 x 24
+// tiles, 2 pixels per thread, 384-thread CTAs (the second staged covariance
+// plane and its four accumulators per patch size need the room).
 cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
-                              int variant) {
-  if (variant == 1) return launch_fast_px<4>(F, d_scenes, grid, st);
-  return launch_fast_px<2>(F, d_scenes, grid, st);
+                              int variant, bool full8) {
+  if (full8) return launch_fast_px<2, kFastTileH8, true>(F, d_scenes, grid, st);
+  if (variant == 1) return launch_fast_px<4, kFastTileH, false>(F, d_scenes, grid, st);
+  return launch_fast_px<2, kFastTileH, false>(F, d_scenes, grid, st);
 }
 
 }  // namespace dcl

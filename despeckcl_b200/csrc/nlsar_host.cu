@@ -103,6 +103,13 @@ static int validate_sizes(int sws, const int* patches, int np, const int* scales
   return DCL_OK;
 }
 
+// DESPECKCL_B200_GENERIC=1 routes every call to the generic kernel (used by
+// the tests to check both kernels against each other)
+static const bool g_force_generic = [] {
+  const char* s = std::getenv("DESPECKCL_B200_GENERIC");
+  return s && s[0] == '1';
+}();
+
 int make_plan(int sws, const int* patches, int np, const int* scales, int ns, const dcl_stats_entry* stats,
               int nstats, float h, float c, int select_mode, bool full8, Plan& pl) {
   std::vector<int> Pv, Sv;
@@ -222,6 +229,10 @@ int make_plan(int sws, const int* patches, int np, const int* scales, int ns, co
   for (size_t si = 0; si < Sv.size(); ++si)
     if (pl.slot_used[si]) pl.shm = std::max(pl.shm, (Sv[si] - 1) / 2);
   F.G = F.wsh + F.phm + pl.shm;
+  // the specialised kernel serves the common settings, in 32 x 32 tiles for
+  // InSAR input and 32 x 24 tiles for 8-plane covariance input
+  pl.fast = !g_force_generic && fast_kernel_supported(F);
+  if (pl.fast && full8) F.tile_h = kFastTileH8;
   return DCL_OK;
 }
 
@@ -357,17 +368,20 @@ int carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d) {
   d.tiles_x = g.tiles_x;
   d.tiles_y = g.tiles_y;
   std::memset(&d.tm_co, 0, sizeof d.tm_co);
+  std::memset(&d.tm_co2, 0, sizeof d.tm_co2);
   std::memset(d.tm_cs, 0, sizeof d.tm_cs);
   if (!uses_specialised_kernel(pl)) return DCL_OK;
   // the specialised kernel stages, per tile, the original covariance box at
   // (vx0 - wsh + G, vy0 - wsh + G) and the scaled covariance box at
   // (vx0 - phm - wsh + G, vy0 - phm - wsh + G), in float4 pixels: x origins
   // in floats are multiples of 4 (16 bytes), as the TMA unit requires
-  const FastStage fs = fast_stage(pl.P.wsh, pl.P.phm);
+  const FastStage fs = fast_stage(pl.P.wsh, pl.P.phm, pl.P.tile_h);
   const uint64_t Hp = (uint64_t)g.Hp, pitch = (uint64_t)g.pitch;
-  int rc = encode_map_2d(&d.tm_co, d.cori, 4 * pitch, Hp, pitch * 16, 4 * fs.RO, fs.RO);
+  int rc = encode_map_2d(&d.tm_co, d.cori, 4 * pitch, Hp, pitch * 16, 4 * fs.RO, fs.ROH);
+  if (rc == DCL_OK && pl.full8) rc = encode_map_2d(&d.tm_co2, d.cori2, 4 * pitch, Hp, pitch * 16, 4 * fs.RO, fs.ROH);
   for (size_t si = 0; si < pl.scales.size() && rc == DCL_OK; ++si)
-    if (pl.slot_used[si]) rc = encode_map_2d(&d.tm_cs[si], d.cs[si], 4 * pitch, Hp, pitch * 16, 4 * fs.RS, fs.RS);
+    if (pl.slot_used[si])
+      rc = encode_map_2d(&d.tm_cs[si], d.cs[si], 4 * pitch, Hp, pitch * 16, 4 * fs.RS, fs.RSH);
   return rc;
 }
 
@@ -380,12 +394,6 @@ struct ProfileState {
   long launches = 0;  // all kernels launched by the library while profiling
 };
 static thread_local ProfileState g_prof;
-// DESPECKCL_B200_GENERIC=1 routes every call to the generic kernel (used by
-// the tests to check both kernels against each other)
-static const bool g_force_generic = [] {
-  const char* s = std::getenv("DESPECKCL_B200_GENERIC");
-  return s && s[0] == '1';
-}();
 
 cudaError_t allow_dynamic_smem(const void* func, size_t bytes, size_t* cache) {
   int dev = 0;
@@ -404,9 +412,7 @@ void profile_count(int n) {
   if (g_prof.on) g_prof.launches += n;
 }
 
-bool uses_specialised_kernel(const Plan& pl) {
-  return !pl.full8 && !g_force_generic && fast_kernel_supported(pl.P);
-}
+bool uses_specialised_kernel(const Plan& pl) { return pl.fast; }
 
 int launch_prep_rows(const Plan& pl, const SceneGeom& g, const SceneDesc& d, const float* a1, const float* a2,
                      const float* phi, const float* cov_in, int co0, int co1, int cs0, int cs1, cudaStream_t st) {
@@ -451,8 +457,8 @@ int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scene
     cudaEventCreate(&b);
     cudaEventRecord(a, st);
   }
-  const bool fast = !pl.full8 && !g_force_generic && fast_kernel_supported(F);
-  const cudaError_t e = fast ? launch_nlsar_fast(F, d_scenes, F.total_tiles, st, variant)
+  const bool fast = pl.fast && fast_kernel_supported(F);
+  const cudaError_t e = fast ? launch_nlsar_fast(F, d_scenes, F.total_tiles, st, variant, pl.full8)
                              : launch_nlsar_fused(pl.full8, F, d_scenes, smem, F.total_tiles, st);
   if (g_prof.on) {
     cudaEventRecord(b, st);
@@ -579,9 +585,15 @@ constexpr int kBandTileRows = 8;  // fewest tile rows per band
 // values of the single-launch path and the results are identical.
 // The downloads are issued after all bands are queued, so a pageable
 // destination (a synchronous copy) still lets the later bands run meanwhile.
-int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const float* phi, float* ref, float* phase,
-                   float* coh, int H, int W) {
-  if (!a1 || !a2 || !phi || !ref || !phase || !coh) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+// `hin` / `hout` are the caller's H x W planes: a1, a2, phi and ref, phase,
+// coh for InSAR inputs (nin = nout = 3), the 8 covariance planes in and out
+// for the covariance path (pl.full8, nin = nout = 8).
+static int run_host_banded(const Plan& pl0, const float* const* hin, int nin, float* const* hout, int nout, int H,
+                           int W) {
+  for (int i = 0; i < nin; ++i)
+    if (!hin[i]) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  for (int i = 0; i < nout; ++i)
+    if (!hout[i]) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
   int dev;
   int rc = ensure_device_ready(dev);
@@ -606,11 +618,12 @@ int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const floa
   const size_t scratch = (scratch_bytes(pl, g) + 255) / 256 * 256;
   const size_t desc_bytes = (nb * sizeof(SceneDesc) + 255) / 256 * 256;
   const size_t wtab_bytes = pl.wtab.size() * sizeof(float);
-  const size_t io_bytes = (6 * b + 255) / 256 * 256;
+  const size_t io_bytes = ((size_t)(nin + nout) * b + 255) / 256 * 256;
   char* mem = nullptr;
   cudaError_t e = cudaMallocAsync(&mem, io_bytes + scratch + desc_bytes + wtab_bytes, st);
   if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io + scratch)");
-  float* buf = reinterpret_cast<float*>(mem);
+  float* buf = reinterpret_cast<float*>(mem);  // [nin][H][W] inputs, then [nout][H][W] outputs
+  float* dout = buf + (size_t)nin * n;
   SceneDesc* d_desc = reinterpret_cast<SceneDesc*>(mem + io_bytes + scratch);
   float* d_wtab = reinterpret_cast<float*>(mem + io_bytes + scratch + desc_bytes);
 
@@ -622,9 +635,13 @@ int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const floa
   rc = carve_scene(pl, g, mem + io_bytes, desc[0]);
   for (int i = 0; i < nb && rc == DCL_OK; ++i) {
     if (i) desc[i] = desc[0];
-    desc[i].ref = buf + 3 * n;
-    desc[i].phase = buf + 4 * n;
-    desc[i].coh = buf + 5 * n;
+    if (pl.full8) {
+      desc[i].cov_out = dout;
+    } else {
+      desc[i].ref = dout;
+      desc[i].phase = dout + n;
+      desc[i].coh = dout + 2 * n;
+    }
     desc[i].tile_begin = 0;
     desc[i].tile_skip = tb[i] * g.tiles_x;
   }
@@ -650,9 +667,8 @@ int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const floa
     const int in_need = last ? H : std::max(1, std::min(H, co_need - G));
     if (in_need > in_done) {
       const size_t off = (size_t)in_done * W, cnt = (size_t)(in_need - in_done) * W * sizeof(float);
-      e = cudaMemcpyAsync(buf + off, a1 + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n + off, a2 + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 2 * n + off, phi + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
+      for (int p = 0; p < nin && e == cudaSuccess; ++p)
+        e = cudaMemcpyAsync(buf + p * n + off, hin[p] + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
       in_done = in_need;
     }
     if (e == cudaSuccess) e = cudaEventRecord(ev_in[i], hp->h2d);
@@ -661,7 +677,10 @@ int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const floa
       rc = cuda_error(e, "cudaMemcpyAsync(H2D)");
       break;
     }
-    launch_prep_rows(pl, g, desc[i], buf, buf + n, buf + 2 * n, nullptr, co_done, co_need, cs_done, cs_need, st);
+    if (pl.full8)
+      launch_prep_rows(pl, g, desc[i], nullptr, nullptr, nullptr, buf, co_done, co_need, cs_done, cs_need, st);
+    else
+      launch_prep_rows(pl, g, desc[i], buf, buf + n, buf + 2 * n, nullptr, co_done, co_need, cs_done, cs_need, st);
     co_done = co_need;
     cs_done = cs_need;
     FilterParams F = pl.P;
@@ -679,9 +698,8 @@ int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const floa
     e = cudaStreamWaitEvent(hp->d2h, ev_out[i], 0);
     if (r1 > r0) {
       const size_t off = (size_t)r0 * W, cnt = (size_t)(r1 - r0) * W * sizeof(float);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(ref + off, buf + 3 * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(phase + off, buf + 4 * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(coh + off, buf + 5 * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
+      for (int p = 0; p < nout && e == cudaSuccess; ++p)
+        e = cudaMemcpyAsync(hout[p] + off, dout + p * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
     }
     if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
   }
@@ -706,32 +724,24 @@ int run_host_insar(const Plan& pl0, const float* a1, const float* a2, const floa
   return rc;
 }
 
+int run_host_insar(const Plan& pl, const float* a1, const float* a2, const float* phi, float* ref, float* phase,
+                   float* coh, int H, int W) {
+  const float* in[3] = {a1, a2, phi};
+  float* out[3] = {ref, phase, coh};
+  return run_host_banded(pl, in, 3, out, 3, H, W);
+}
+
 int run_host_covmat(const Plan& pl, const float* cin, float* cout, int H, int W) {
   if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
-  int dev;
-  int rc = ensure_device_ready(dev);
-  if (rc) return rc;
-  cudaStream_t st = cudaStreamPerThread;
-  const size_t n = (size_t)8 * H * W, b = n * sizeof(float);
-  float* buf = nullptr;
-  cudaError_t e = cudaMallocAsync(&buf, 2 * b, st);
-  if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io)");
-  e = cudaMemcpyAsync(buf, cin, b, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    cudaFreeAsync(buf, st);
-    return cuda_error(e, "cudaMemcpyAsync(H2D)");
+  const size_t n = (size_t)H * W;
+  const float* in[8];
+  float* out[8];
+  for (int p = 0; p < 8; ++p) {
+    in[p] = cin + p * n;
+    out[p] = cout + p * n;
   }
-  SceneIO s{nullptr, nullptr, nullptr, buf, nullptr, nullptr, nullptr, buf + n, nullptr, H, W};
-  rc = run_device(pl, {s}, st);
-  if (rc == DCL_OK) {
-    e = cudaMemcpyAsync(cout, buf + n, b, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
-  }
-  cudaFreeAsync(buf, st);
-  cudaError_t e2 = cudaStreamSynchronize(st);
-  if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR");
-  return rc;
+  return run_host_banded(pl, in, 8, out, 8, H, W);
 }
 
 }  // namespace dcl

@@ -20,6 +20,7 @@ struct Plan {
   int overlap = 0;
   int shm = 0;                   // largest scale half among used slots
   bool full8 = false;
+  bool fast = false;  // served by the specialised kernel (nlsar_fast.cu)
   int px = 4;
 };
 

@@ -213,6 +213,42 @@ def test_specialised_and_generic_kernels_agree(tmp_path, train_stats):
     assert (wrapped(fast[1] - gen[1]) <= 1e-3).mean() >= 0.99
 
 
+@pytest.mark.parametrize("mode", ["argmax_enl", "reference"])
+def test_covariance_specialised_and_generic_kernels_agree(tmp_path, oracle, train_stats, mode):
+    # 8-plane covariance input: the specialised kernel (32 x 24 tiles) against
+    # the generic one, forced in a child process, up to FP32 summation order
+    import os
+    import pickle
+    import subprocess
+    import sys
+
+    a1, a2, ph = synthetic.insar_scene(75, 90, 31)
+    cov8 = oracle.covmat_create(a1, a2, ph).astype(np.float32)
+    rng = np.random.default_rng(5)
+    cov8[1] = rng.normal(0, 0.1, cov8[1].shape)
+    cov8[7] = rng.normal(0, 0.1, cov8[7].shape)
+    cov8[4] *= 1.02
+    cplx = (cov8[0::2] + 1j * cov8[1::2]).reshape(2, 2, 75, 90)
+    fast = dcl.nlsar(cplx, SWS, PATCHES, SCALES, train_stats, select_mode=mode)
+    f = tmp_path / "in.pkl"
+    stats = {k: (v.lut_size, v.dissims_min, v.dissims_max, v.quantilles, v.chi2cdf_inv)
+             for k, v in train_stats.items()}
+    pickle.dump((cplx, stats), open(f, "wb"))
+    code = (
+        "import pickle,sys,numpy as np; sys.path.insert(0, %r); import despeckcl_b200 as d; "
+        "c,st=pickle.load(open(%r,'rb')); "
+        "st={k: d.Stats(*v) for k,v in st.items()}; "
+        "r=d.nlsar(c,21,[3,5,7],[1,3],st,select_mode=%r); "
+        "pickle.dump(r, open(%r,'wb'))" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), str(f),
+                                          mode, str(tmp_path / "out.pkl")))
+    env = dict(os.environ, DESPECKCL_B200_GENERIC="1")
+    subprocess.run([sys.executable, "-c", code], env=env, check=True)
+    gen = pickle.load(open(tmp_path / "out.pkl", "rb"))
+    scale = np.maximum(np.abs(gen), np.abs(gen[0, 0]).real[None, None] * 1e-2)
+    err = np.abs(fast - gen) / scale
+    assert (err <= 1e-4).mean() >= 0.99, err.max()
+
+
 def test_host_entry_point_equals_device_entry_point(train_stats):
     a1, a2, ph = synthetic.insar_scene(70, 90, 10)
     host = dcl.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode="argmax_enl")
@@ -231,6 +267,32 @@ def test_banded_host_entry_point_equals_device_entry_point(train_stats, shape, m
     dev = run_gpu(a1, a2, ph, train_stats, mode)
     for h, d in zip(host, dev):
         np.testing.assert_array_equal(h, d)
+
+
+@pytest.mark.parametrize("shape", [(530, 70), (1045, 45)])
+def test_banded_covariance_host_entry_point_equals_device_entry_point(oracle, train_stats, shape):
+    import ctypes
+
+    import despeckcl_b200.api as api
+
+    H, W = shape
+    a1, a2, ph = synthetic.insar_scene(H, W, 22)
+    cov8 = np.ascontiguousarray(oracle.covmat_create(a1, a2, ph), dtype=np.float32)
+    cov8[1] = np.random.default_rng(1).normal(0, 0.1, cov8[1].shape)
+    L = api.lib()
+    pk, pp, npn = api._ints(PATCHES)
+    sk, sp, nsn = api._ints(SCALES)
+    arr, n, keep = api._entries(train_stats)
+    host = np.empty_like(cov8)
+    api._check(L.dcl_nlsar_covmat(api._fp(cov8), api._fp(host), H, W, 2, SWS, pp, npn, sp, nsn, arr, n,
+                                  ctypes.c_float(15.0), ctypes.c_float(49.0), 1))
+    din = torch.from_numpy(cov8).cuda()
+    dout = torch.empty_like(din)
+    api._check(L.dcl_nlsar_covmat_device(ctypes.c_void_p(din.data_ptr()), ctypes.c_void_p(dout.data_ptr()), H, W, 2,
+                                         SWS, pp, npn, sp, nsn, arr, n, ctypes.c_float(15.0), ctypes.c_float(49.0), 1,
+                                         None))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(host, dout.cpu().numpy())
 
 
 def test_shift_invariance_is_bit_exact(train_stats):
