@@ -450,14 +450,17 @@ def test_training_3x3_matches_oracle(oracle):
 
 
 @pytest.mark.parametrize("mode", ["reference", "argmax_enl"])
-def test_covariance_3x3_path_matches_oracle(oracle, mode):
+@pytest.mark.parametrize("sws,patches", [(SWS, PATCHES), (15, [3, 5])])
+def test_covariance_3x3_path_matches_oracle(oracle, mode, sws, patches):
+    # search 21 with patches {3,5,7} runs the specialised 3x3 kernel, search
+    # 15 with {3,5} the generic one
     tp, _ = _polsar_scene(40, 40, 41, homogeneous=True)
     stats = oracle.training_covmat(tp, [3, 5, 7], [1, 3])
     planes, cplx = _polsar_scene(44, 60, 42)
     m = 0 if mode == "reference" else 1
-    o = oracle.nlsar_covmat(planes, SWS, PATCHES, SCALES, stats, select_mode=m, use_double=True)
-    o32 = oracle.nlsar_covmat(planes, SWS, PATCHES, SCALES, stats, select_mode=m)
-    g = dcl.nlsar(cplx, SWS, PATCHES, SCALES, stats, select_mode=mode)
+    o = oracle.nlsar_covmat(planes, sws, patches, SCALES, stats, select_mode=m, use_double=True)
+    o32 = oracle.nlsar_covmat(planes, sws, patches, SCALES, stats, select_mode=m)
+    g = dcl.nlsar(cplx, sws, patches, SCALES, stats, select_mode=mode)
     gi = np.empty_like(o)
     gi[0::2] = g.real.reshape(9, 44, 60)
     gi[1::2] = g.imag.reshape(9, 44, 60)
