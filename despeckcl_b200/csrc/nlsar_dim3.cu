@@ -28,7 +28,9 @@
 // vertical sums, the composite LUT weight and 23 accumulators per patch size
 // (sum w, w^2, w I_d^2 for d = 0..2, and w times each of the 18 planes, read
 // through the L1 cache); the epilogue derives ENL, alpha and ENL', selects and
-// blends with the centre pixel.
+// blends with the centre pixel.  Search 21 with patches {3,5,7} (or one of
+// them) runs nlsar3_fast_kernel instead, which splits each pixel's
+// accumulators over two threads.
 
 #include <cuda_runtime.h>
 
