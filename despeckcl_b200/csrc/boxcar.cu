@@ -106,17 +106,37 @@ __global__ void __launch_bounds__(kBoxThreads)
   float* sHs = sm + 3 * SH * SW;     // [3][SH][kBoxTW] horizontal sums
   const int vy0 = blockIdx.y * kBoxTH, vx0 = blockIdx.x * kBoxTW;
   const int tid = threadIdx.x;
-  for (int i = tid; i < SH * SW; i += kBoxThreads) {
-    const int rr = i / SW, cc = i - rr * SW;
-    const int y = clampi_b(vy0 - R + rr, 0, H - 1), x = clampi_b(vx0 - R + cc, 0, W - 1);
-    const size_t g = (size_t)y * W + x;
-    const float am = a1[g], as = a2[g];
-    float sn, cs;
-    __sincosf(phi[g], &sn, &cs);
-    const float aa = am * as;
-    sIn[i] = (am * am + as * as) / 2;
-    sIn[SH * SW + i] = aa * cs;
-    sIn[2 * SH * SW + i] = aa * sn;
+  // staging: each thread issues the loads of U pixels (all of its share, up
+  // to 12) before using any of them, so up to 3U loads per thread are in
+  // flight (the staging is bound by memory latency, not bandwidth, at one
+  // load in flight per plane)
+  constexpr int U = (SH * SW + kBoxThreads - 1) / kBoxThreads < 12 ? (SH * SW + kBoxThreads - 1) / kBoxThreads : 12;
+  for (int i0 = tid; i0 < SH * SW; i0 += U * kBoxThreads) {
+    float am[U], as[U], ph[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * kBoxThreads;
+      if (i < SH * SW) {
+        const int rr = i / SW, cc = i - rr * SW;
+        const int y = clampi_b(vy0 - R + rr, 0, H - 1), x = clampi_b(vx0 - R + cc, 0, W - 1);
+        const size_t g = (size_t)y * W + x;
+        am[u] = __ldg(a1 + g);
+        as[u] = __ldg(a2 + g);
+        ph[u] = __ldg(phi + g);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * kBoxThreads;
+      if (i < SH * SW) {
+        float sn, cs;
+        __sincosf(ph[u], &sn, &cs);
+        const float aa = am[u] * as[u];
+        sIn[i] = (am[u] * am[u] + as[u] * as[u]) / 2;
+        sIn[SH * SW + i] = aa * cs;
+        sIn[2 * SH * SW + i] = aa * sn;
+      }
+    }
   }
   __syncthreads();
   // horizontal: item = (plane, row, group of 4 columns)
