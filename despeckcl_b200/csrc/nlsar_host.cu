@@ -572,8 +572,9 @@ static int host_pipe(int dev, size_t nev, HostPipe*& out) {
   return DCL_OK;
 }
 
-constexpr int kMaxBands = 8;      // row bands of a host-pointer call
-constexpr int kBandTileRows = 8;  // fewest tile rows per band
+constexpr int kMaxBands = 8;   // row bands of a host-pointer call
+constexpr int kBandWaves = 8;  // fewest waves of tiles (one CTA per SM) per band: each band's launch
+                               // ends in a partly filled wave, so small scenes stay in one band
 
 // Host pointers: the reference's filter_sub_image uploads the inputs and
 // downloads the results around its kernels (nlsar/conversion.cpp:22-142).
@@ -605,7 +606,17 @@ static int run_host_banded(const Plan& pl0, const float* const* hin, int nin, fl
   pl.P.K = K;
   const SceneGeom g = scene_geom(pl, H, W);
   if ((long long)g.tiles_x * g.tiles_y > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
-  const int nb = std::max(1, std::min(kMaxBands, g.tiles_y / kBandTileRows));
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  const long long tiles = (long long)g.tiles_x * g.tiles_y;
+  int nb = (int)std::max(1LL, std::min<long long>(std::min(kMaxBands, g.tiles_y),
+                                                  tiles / ((long long)kBandWaves * sms)));
+  // DESPECKCL_B200_BANDS=n forces n bands (at most one per tile row): the
+  // tests use it to cut small scenes
+  if (const char* fb = std::getenv("DESPECKCL_B200_BANDS")) {
+    const int n = std::atoi(fb);
+    if (n > 0) nb = std::min(n, g.tiles_y);
+  }
   HostPipe* hp = nullptr;
   rc = host_pipe(dev, 2 * (size_t)nb + 2, hp);
   if (rc) return rc;

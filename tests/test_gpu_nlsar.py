@@ -257,11 +257,15 @@ def test_host_entry_point_equals_device_entry_point(train_stats):
         np.testing.assert_array_equal(h, d)
 
 
-@pytest.mark.parametrize("shape,mode", [((1061, 97), "argmax_enl"), ((520, 64), "reference"),
-                                        ((777, 41), "argmax_enl")])
-def test_banded_host_entry_point_equals_device_entry_point(train_stats, shape, mode):
-    # scenes of 16+ tile rows go through the host entry point in row bands
-    # whose copies overlap the filtering; results must equal one launch's
+@pytest.mark.parametrize("shape,mode,bands", [((1061, 97), "argmax_enl", 4), ((520, 64), "reference", 2),
+                                              ((777, 41), "argmax_enl", 25), ((1700, 1500), "argmax_enl", None)])
+def test_banded_host_entry_point_equals_device_entry_point(train_stats, monkeypatch, shape, mode, bands):
+    # the host entry point filters scenes of many waves of tiles in row bands
+    # whose copies overlap the filtering (1700 x 1500: two bands by itself;
+    # the smaller scenes are cut by DESPECKCL_B200_BANDS); results must equal
+    # one launch's
+    if bands is not None:
+        monkeypatch.setenv("DESPECKCL_B200_BANDS", str(bands))
     a1, a2, ph = synthetic.insar_scene(*shape, 21)
     host = dcl.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=mode)
     dev = run_gpu(a1, a2, ph, train_stats, mode)
@@ -269,12 +273,13 @@ def test_banded_host_entry_point_equals_device_entry_point(train_stats, shape, m
         np.testing.assert_array_equal(h, d)
 
 
-@pytest.mark.parametrize("shape", [(530, 70), (1045, 45)])
-def test_banded_covariance_host_entry_point_equals_device_entry_point(oracle, train_stats, shape):
+@pytest.mark.parametrize("shape,bands", [((530, 70), 2), ((1045, 45), 5)])
+def test_banded_covariance_host_entry_point_equals_device_entry_point(oracle, train_stats, monkeypatch, shape, bands):
     import ctypes
 
     import despeckcl_b200.api as api
 
+    monkeypatch.setenv("DESPECKCL_B200_BANDS", str(bands))
     H, W = shape
     a1, a2, ph = synthetic.insar_scene(H, W, 22)
     cov8 = np.ascontiguousarray(oracle.covmat_create(a1, a2, ph), dtype=np.float32)
