@@ -2,10 +2,11 @@
 // half size and the patch half sizes of a pass (the common configurations),
 // for sm_100a.  Same semantics as the generic kernel in nlsar_kernels.cu.
 //
-// Per CTA: a 32 x 32 output tile, each thread owning 2 (16 warps) or 4 (8 warps)
-// vertically consecutive pixels of one column.  For every scale the search-window offsets
-// are taken three at a time along a row of the window (same dy, consecutive
-// dx, so a thread's neighbour loads overlap across the batch):
+// Per CTA: a 32 x 32 output tile (32 x 24 for 8-plane covariance input), each
+// thread owning 2 (16 warps) or 4 (8 warps) vertically consecutive pixels of
+// one column.  For every scale the search-window offsets are taken three at a
+// time (seven when a pass has one patch size) along a row of the window (same
+// dy, consecutive dx, so a thread's neighbour loads overlap across the batch):
 //   A  GLR similarities of the batch on the tile plus the patch halo
 //      (each thread: one pixel x three offsets); the measure is evaluated in
 //      an order symmetric in its two pixels, so the mirrored half window gets
@@ -45,7 +46,9 @@ struct Fast {
   static constexpr bool FULL8 = FULL8_;              // 8-plane covariance input and output
   static constexpr int TH = TH_, TW = 32, PX = PX_;  // tile rows; vertically adjacent pixels per thread
   static constexpr int WARPS = TH / PX, THREADS = 32 * WARPS;
-  static constexpr int K = 3;                        // offsets per batch (SWS % K == 0)
+  // offsets per batch (SWS % K == 0): a single patch size leaves shared
+  // memory for seven, which amortises phase A's centre loads and the barriers
+  static constexpr int K = NP == 1 ? 7 : 3;
   static constexpr int NA = FULL8 ? 12 : 8;          // accumulators per (pixel, patch size)
   static constexpr int NM = FULL8 ? 8 : 4;           // weighted sums kept for the selected combination
   static constexpr int RS = TW + 2 * (PHM + WSH);    // scaled covariance region: RS x RSH
