@@ -80,6 +80,7 @@ struct Scene3 {
   const float* ld[kMaxScales];  // [Hp][pitch] per scale slot
   float* out;                   // [18][H][W]
   int H, W, vH, vW, pitch, tiles_x;
+  int tile_skip;                // scene tiles before block 0 of the launch (row bands)
   size_t plane;                 // Hp * pitch
 };
 
@@ -109,10 +110,10 @@ __host__ __device__ inline Smem3 smem3_layout(int wsh, int phm, int K) {
 
 // 18 planes of the clamp-padded frame (sub_images.cpp:37-38 clamping)
 __global__ void prep3_cov_kernel(const float* __restrict__ cin, int H, int W, float* __restrict__ c18, int Hp, int Wp,
-                                 int pitch, size_t plane, int G) {
+                                 int pitch, size_t plane, int G, int row0, int row1) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
-  const int py = blockIdx.y * blockDim.y + threadIdx.y;
-  if (px >= Wp || py >= Hp) return;
+  const int py = row0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= row1) return;
   const int y = clamp3(py - G, 0, H - 1), x = clamp3(px - G, 0, W - 1);
   const size_t n = (size_t)H * W, i = (size_t)y * W + x, o = (size_t)py * pitch + px;
 #pragma unroll
@@ -123,10 +124,11 @@ __global__ void prep3_cov_kernel(const float* __restrict__ cin, int H, int W, fl
 // averaged (covmat_spatial_avg.cl:50-57) similarity planes of one scale, and
 // their ln det
 __global__ void prep3_scale_kernel(const float* __restrict__ c18, int Hp, int Wp, int pitch, size_t plane, int s,
-                                   GaussArg ga, float gamma, float* __restrict__ s9, float* __restrict__ ld) {
+                                   GaussArg ga, float gamma, float* __restrict__ s9, float* __restrict__ ld, int row0,
+                                   int row1) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
-  const int py = blockIdx.y * blockDim.y + threadIdx.y;
-  if (px >= Wp || py >= Hp) return;
+  const int py = row0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= Wp || py >= row1) return;
   const int ssh = (s - 1) / 2;
   float a[9];
 #pragma unroll
@@ -177,7 +179,8 @@ __global__ void __launch_bounds__(kT3Threads, 1) nlsar3_kernel(const FilterParam
   float* sSim = smem + L.off_sim;
   float* sH = smem + L.off_h;
   float* sW = smem + L.off_w;
-  const int ty = blockIdx.x / S.tiles_x, tx = blockIdx.x - ty * S.tiles_x;
+  const int lt = blockIdx.x + S.tile_skip;
+  const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
   const int vy0 = ty * kT3H, vx0 = tx * kT3W;
   // frame index of this thread's output pixel
   const size_t cfi = (size_t)(vy0 + y + G) * S.pitch + (vx0 + lane + G);
@@ -446,7 +449,8 @@ __global__ void __launch_bounds__(Fast3<PH0, PH1, PH2>::THREADS, 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp / C::TH, y = warp - grp * C::TH;  // warp-uniform group, output row
   const int px = y * 32 + lane;
-  const int ty = blockIdx.x / S.tiles_x, tx = blockIdx.x - ty * S.tiles_x;
+  const int lt = blockIdx.x + S.tile_skip;
+  const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
   const int vy0 = ty * C::TH, vx0 = tx * TW;
   const int G = P.G;
   const size_t cfi = (size_t)(vy0 + y + G) * S.pitch + (vx0 + lane + G);
@@ -784,99 +788,144 @@ float rescale_gamma_3x3() {
 
 }  // namespace
 
-// NL-SAR of one 3x3 covariance scene on device pointers (planes [18][H][W]).
-int nlsar_covmat3_device(const Plan& pl0, const float* cin, float* cout, int H, int W, cudaStream_t st) {
-  if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
-  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+// A planned 3x3 call: kernel parameters, frame geometry and scratch (frames
+// and the weight table, allocated on the call's stream).
+struct Run3 {
+  Plan pl;
+  Scene3 S;
+  size_t smem = 0;
+  int tiles_y = 0, Hp = 0, Wp = 0, used = 0;
+  char* scratch = nullptr;
+};
+
+static int plan3(const Plan& pl0, int H, int W, float* cout, Run3& r, cudaStream_t st) {
   int dev = 0;
   int rc = ensure_device_ready(dev);
   if (rc) return rc;
-  Plan pl = pl0;
-  FilterParams& F = pl.P;
+  r.pl = pl0;
+  FilterParams& F = r.pl.P;
   F.c2d = 2 * 3 * std::log(2.0f);
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || optin <= 0)
     optin = 227 * 1024;
   int K = 0;
-  size_t smem = 0;
   for (int k = 8; k >= 1 && K == 0; --k) {
     const size_t b = (size_t)smem3_layout(F.wsh, F.phm, k).total * 4;
     if (b <= (size_t)optin) {
       K = k;
-      smem = b;
+      r.smem = b;
     }
   }
   if (K < 1) return set_error(DCL_ERR_UNSUPPORTED, "search window / patch sizes too large for shared memory");
   F.K = K;
   F.tile_h = kT3H;
-
-  Scene3 S;
+  Scene3& S = r.S;
   std::memset(&S, 0, sizeof S);
   S.H = H;
   S.W = W;
-  S.vH = H - 1 + pl.overlap;
-  S.vW = W - 1 + pl.overlap;
-  const int tiles_y = (S.vH + 1 + kT3H - 1) / kT3H;
+  S.vH = H - 1 + r.pl.overlap;
+  S.vW = W - 1 + r.pl.overlap;
+  r.tiles_y = (S.vH + 1 + kT3H - 1) / kT3H;
   S.tiles_x = (S.vW + 1 + kT3W - 1) / kT3W;
-  const int Hp = tiles_y * kT3H + 2 * F.G, Wp = S.tiles_x * kT3W + 2 * F.G;
-  S.pitch = (Wp + 7) / 8 * 8;
-  S.plane = (size_t)Hp * S.pitch;
-  const long long tiles = (long long)tiles_y * S.tiles_x;
-  if (tiles > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
-  int used = 0;
-  for (char u : pl.slot_used) used += u ? 1 : 0;
-  const size_t frame_bytes = S.plane * sizeof(float) * (18 + 10 * (size_t)used);
-  const size_t wtab_bytes = pl.wtab.size() * sizeof(float);
-  char* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, frame_bytes + wtab_bytes + 256, st);
+  r.Hp = r.tiles_y * kT3H + 2 * F.G;
+  r.Wp = S.tiles_x * kT3W + 2 * F.G;
+  S.pitch = (r.Wp + 7) / 8 * 8;
+  S.plane = (size_t)r.Hp * S.pitch;
+  if ((long long)r.tiles_y * S.tiles_x > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
+  r.used = 0;
+  for (char u : r.pl.slot_used) r.used += u ? 1 : 0;
+  const size_t frame_bytes = S.plane * sizeof(float) * (18 + 10 * (size_t)r.used);
+  const size_t wtab_bytes = r.pl.wtab.size() * sizeof(float);
+  cudaError_t e = cudaMallocAsync(&r.scratch, frame_bytes + wtab_bytes + 256, st);
   if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(3x3 scratch)");
-  float* p = reinterpret_cast<float*>(scratch);
+  float* p = reinterpret_cast<float*>(r.scratch);
   S.c18 = p;
   p += 18 * S.plane;
-  for (size_t si = 0; si < pl.scales.size(); ++si)
-    if (pl.slot_used[si]) {
+  for (size_t si = 0; si < r.pl.scales.size(); ++si)
+    if (r.pl.slot_used[si]) {
       S.s9[si] = p;
       p += 9 * S.plane;
       S.ld[si] = p;
       p += S.plane;
     }
-  float* d_wtab = reinterpret_cast<float*>(scratch + (frame_bytes + 255) / 256 * 256);
+  float* d_wtab = reinterpret_cast<float*>(r.scratch + (frame_bytes + 255) / 256 * 256);
   S.out = cout;
-  e = cudaMemcpyAsync(d_wtab, pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice, st);
+  e = cudaMemcpyAsync(d_wtab, r.pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(3x3 weights)");
   F.wtab = d_wtab;
   F.n_scenes = 1;
-  F.total_tiles = (int)tiles;
-  if (e == cudaSuccess) {
-    dim3 blk(32, 8), grd((Wp + 31) / 32, (Hp + 7) / 8);
-    prep3_cov_kernel<<<grd, blk, 0, st>>>(cin, H, W, const_cast<float*>(S.c18), Hp, Wp, S.pitch, S.plane, F.G);
-    const float gamma = rescale_gamma_3x3();
-    for (size_t si = 0; si < pl.scales.size(); ++si) {
-      if (!pl.slot_used[si]) continue;
-      GaussArg ga;
-      std::memset(&ga, 0, sizeof ga);
-      const std::vector<float> gw = gauss_weights(pl.scales[si]);
-      std::copy(gw.begin(), gw.end(), ga.g);
-      prep3_scale_kernel<<<grd, blk, 0, st>>>(S.c18, Hp, Wp, S.pitch, S.plane, pl.scales[si], ga, gamma,
-                                              const_cast<float*>(S.s9[si]), const_cast<float*>(S.ld[si]));
-    }
-    if (pl.fast) {
-      e = launch3_fast(F, S, (unsigned)tiles, st);
-    } else {
-      static size_t allowed[kMaxDevices];
-      e = allow_dynamic_smem((const void*)nlsar3_kernel, smem, allowed);
-      if (e == cudaSuccess) {
-        nlsar3_kernel<<<(unsigned)tiles, kT3Threads, smem, st>>>(F, S);
-        e = cudaGetLastError();
-      }
-    }
-    profile_count(2 + used);
-  }
-  cudaFreeAsync(scratch, st);
-  if (e != cudaSuccess) return cuda_error(e, "NL-SAR 3x3");
   return DCL_OK;
 }
 
-// Host pointers: copy in, run, copy out.
+// frame rows [co0, co1) of the covariance planes and [cs0, cs1) of every
+// scale's similarity planes (the rows those read must be filled already)
+static int prep3_rows(const Run3& r, const float* cin, int co0, int co1, int cs0, int cs1, cudaStream_t st) {
+  const FilterParams& F = r.pl.P;
+  const Scene3& S = r.S;
+  const dim3 blk(32, 8);
+  const unsigned gx = (unsigned)(r.Wp + 31) / 32;
+  if (co1 > co0) {
+    prep3_cov_kernel<<<dim3(gx, (unsigned)(co1 - co0 + 7) / 8), blk, 0, st>>>(
+        cin, S.H, S.W, const_cast<float*>(S.c18), r.Hp, r.Wp, S.pitch, S.plane, F.G, co0, co1);
+    profile_count(1);
+  }
+  if (cs1 > cs0) {
+    const float gamma = rescale_gamma_3x3();
+    for (size_t si = 0; si < r.pl.scales.size(); ++si) {
+      if (!r.pl.slot_used[si]) continue;
+      GaussArg ga;
+      std::memset(&ga, 0, sizeof ga);
+      const std::vector<float> gw = gauss_weights(r.pl.scales[si]);
+      std::copy(gw.begin(), gw.end(), ga.g);
+      prep3_scale_kernel<<<dim3(gx, (unsigned)(cs1 - cs0 + 7) / 8), blk, 0, st>>>(
+          S.c18, r.Hp, r.Wp, S.pitch, S.plane, r.pl.scales[si], ga, gamma, const_cast<float*>(S.s9[si]),
+          const_cast<float*>(S.ld[si]), cs0, cs1);
+      profile_count(1);
+    }
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? DCL_OK : cuda_error(e, "NL-SAR 3x3 prep");
+}
+
+// the fused kernel on tile rows [t0, t1)
+static int launch3_rows(const Run3& r, int t0, int t1, cudaStream_t st) {
+  if (t1 <= t0) return DCL_OK;
+  Scene3 S = r.S;
+  S.tile_skip = t0 * S.tiles_x;
+  FilterParams F = r.pl.P;
+  const unsigned tiles = (unsigned)((t1 - t0) * S.tiles_x);
+  F.total_tiles = (int)tiles;
+  cudaError_t e;
+  if (r.pl.fast) {
+    e = launch3_fast(F, S, tiles, st);
+  } else {
+    static size_t allowed[kMaxDevices];
+    e = allow_dynamic_smem((const void*)nlsar3_kernel, r.smem, allowed);
+    if (e == cudaSuccess) {
+      nlsar3_kernel<<<tiles, kT3Threads, r.smem, st>>>(F, S);
+      e = cudaGetLastError();
+    }
+  }
+  profile_count(1);
+  return e == cudaSuccess ? DCL_OK : cuda_error(e, "NL-SAR 3x3");
+}
+
+// NL-SAR of one 3x3 covariance scene on device pointers (planes [18][H][W]).
+int nlsar_covmat3_device(const Plan& pl, const float* cin, float* cout, int H, int W, cudaStream_t st) {
+  if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
+  if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
+  Run3 r;
+  int rc = plan3(pl, H, W, cout, r, st);
+  if (rc == DCL_OK) rc = prep3_rows(r, cin, 0, r.Hp, 0, r.Hp, st);
+  if (rc == DCL_OK) rc = launch3_rows(r, 0, r.tiles_y, st);
+  if (r.scratch) cudaFreeAsync(r.scratch, st);
+  return rc;
+}
+
+// Host pointers, in row bands as the 2x2 host calls: band b's input rows go
+// up on a copy stream while band b-1 is filtered, its results come down on a
+// second one; frame rows are filled only where their inputs have arrived, so
+// the results equal the device entry point's.
 int nlsar_covmat3_host(const Plan& pl, const float* cin, float* cout, int H, int W) {
   if (!cin || !cout) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
   if (H < 1 || W < 1) return set_error(DCL_ERR_INVALID_ARGUMENT, "height and width must be >= 1");
@@ -884,23 +933,78 @@ int nlsar_covmat3_host(const Plan& pl, const float* cin, float* cout, int H, int
   int rc = ensure_device_ready(dev);
   if (rc) return rc;
   cudaStream_t st = cudaStreamPerThread;
-  const size_t n = (size_t)18 * H * W, b = n * sizeof(float);
+  const size_t n = (size_t)H * W;
   float* buf = nullptr;
-  cudaError_t e = cudaMallocAsync(&buf, 2 * b, st);
+  cudaError_t e = cudaMallocAsync(&buf, 2 * 18 * n * sizeof(float), st);
   if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io)");
-  e = cudaMemcpyAsync(buf, cin, b, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    cudaFreeAsync(buf, st);
-    return cuda_error(e, "cudaMemcpyAsync(H2D)");
-  }
-  rc = nlsar_covmat3_device(pl, buf, buf + n, H, W, st);
+  float* dout = buf + 18 * n;
+  Run3 r;
+  rc = plan3(pl, H, W, dout, r, st);
+  const int nb = rc == DCL_OK ? band_count(dev, (long long)r.tiles_y * r.S.tiles_x, r.tiles_y) : 1;
+  HostPipe* hp = nullptr;
+  if (rc == DCL_OK) rc = host_pipe(dev, 2 * (size_t)nb + 2, hp);
   if (rc == DCL_OK) {
-    e = cudaMemcpyAsync(cout, buf + n, b, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
+    cudaEvent_t* ev_in = hp->ev.data();
+    cudaEvent_t* ev_out = hp->ev.data() + nb;
+    cudaEvent_t ev_alloc = hp->ev[2 * nb];
+    e = cudaEventRecord(ev_alloc, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp->h2d, ev_alloc, 0);
+    if (e != cudaSuccess) rc = cuda_error(e, "event");
+    std::vector<int> tb(nb + 1);
+    for (int i = 0; i <= nb; ++i) tb[i] = (int)((long long)r.tiles_y * i / nb);
+    const FilterParams& F = r.pl.P;
+    int in_done = 0, co_done = 0, cs_done = 0;
+    for (int i = 0; i < nb && rc == DCL_OK; ++i) {
+      const bool last = i == nb - 1;
+      const int cs_need = last ? r.Hp : std::min(r.Hp, tb[i + 1] * kT3H + F.phm + F.wsh + F.G);
+      const int co_need = last ? r.Hp : std::min(r.Hp, cs_need + r.pl.shm);
+      const int in_need = last ? H : std::max(1, std::min(H, co_need - F.G));
+      if (in_need > in_done) {
+        const size_t off = (size_t)in_done * W, cnt = (size_t)(in_need - in_done) * W * sizeof(float);
+        for (int p = 0; p < 18 && e == cudaSuccess; ++p)
+          e = cudaMemcpyAsync(buf + p * n + off, cin + p * n + off, cnt, cudaMemcpyHostToDevice, hp->h2d);
+        in_done = in_need;
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(ev_in[i], hp->h2d);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev_in[i], 0);
+      if (e != cudaSuccess) {
+        rc = cuda_error(e, "cudaMemcpyAsync(H2D)");
+        break;
+      }
+      rc = prep3_rows(r, buf, co_done, co_need, cs_done, cs_need, st);
+      co_done = co_need;
+      cs_done = cs_need;
+      if (rc == DCL_OK) rc = launch3_rows(r, tb[i], tb[i + 1], st);
+      if (rc == DCL_OK && (e = cudaEventRecord(ev_out[i], st)) != cudaSuccess) rc = cuda_error(e, "event");
+    }
+    // band b holds output rows [tb[b] * 8, tb[b+1] * 8) below row H-1; row
+    // H-1 comes from the last tile row
+    for (int i = 0; i < nb && rc == DCL_OK; ++i) {
+      const int r0 = std::min(tb[i] * kT3H, H - 1);
+      const int r1 = i == nb - 1 ? H : std::min(tb[i + 1] * kT3H, H - 1);
+      e = cudaStreamWaitEvent(hp->d2h, ev_out[i], 0);
+      if (r1 > r0) {
+        const size_t off = (size_t)r0 * W, cnt = (size_t)(r1 - r0) * W * sizeof(float);
+        for (int p = 0; p < 18 && e == cudaSuccess; ++p)
+          e = cudaMemcpyAsync(cout + p * n + off, dout + p * n + off, cnt, cudaMemcpyDeviceToHost, hp->d2h);
+      }
+      if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(D2H)");
+    }
+    // free in stream order after every copy
+    cudaEvent_t ev_done = hp->ev[2 * nb + 1];
+    cudaError_t e2 = cudaEventRecord(ev_done, hp->d2h);
+    if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(st, ev_done, 0);
+    cudaError_t e3 = cudaEventRecord(ev_done, hp->h2d);
+    if (e3 == cudaSuccess) e3 = cudaStreamWaitEvent(st, ev_done, 0);
+    if (e2 != cudaSuccess || e3 != cudaSuccess) {
+      cudaStreamSynchronize(hp->h2d);
+      cudaStreamSynchronize(hp->d2h);
+    }
   }
+  if (r.scratch) cudaFreeAsync(r.scratch, st);
   cudaFreeAsync(buf, st);
-  const cudaError_t e2 = cudaStreamSynchronize(st);
-  if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR 3x3");
+  const cudaError_t e4 = cudaStreamSynchronize(st);
+  if (rc == DCL_OK && e4 != cudaSuccess) rc = cuda_error(e4, "NL-SAR 3x3");
   return rc;
 }
 

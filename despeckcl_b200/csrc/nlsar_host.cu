@@ -550,13 +550,9 @@ int run_device(const Plan& pl0, const std::vector<SceneIO>& io, cudaStream_t st)
 
 // Copy streams and events of the calling thread's host-pointer calls, one
 // set per device, created on first use and kept for the thread's lifetime.
-struct HostPipe {
-  cudaStream_t h2d = nullptr, d2h = nullptr;
-  std::vector<cudaEvent_t> ev;
-};
 static thread_local HostPipe g_pipes[kMaxDevices];
 
-static int host_pipe(int dev, size_t nev, HostPipe*& out) {
+int host_pipe(int dev, size_t nev, HostPipe*& out) {
   if (dev < 0 || dev >= kMaxDevices) return set_error(DCL_ERR_CUDA, "device %d out of range", dev);
   HostPipe& p = g_pipes[dev];
   cudaError_t e = cudaSuccess;
@@ -575,6 +571,20 @@ static int host_pipe(int dev, size_t nev, HostPipe*& out) {
 constexpr int kMaxBands = 8;   // row bands of a host-pointer call
 constexpr int kBandWaves = 8;  // fewest waves of tiles (one CTA per SM) per band: each band's launch
                                // ends in a partly filled wave, so small scenes stay in one band
+
+int band_count(int dev, long long tiles, int tile_rows) {
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  int nb = (int)std::max(1LL, std::min<long long>(std::min(kMaxBands, tile_rows),
+                                                  tiles / ((long long)kBandWaves * sms)));
+  // DESPECKCL_B200_BANDS=n forces n bands (at most one per tile row): the
+  // tests use it to cut small scenes
+  if (const char* fb = std::getenv("DESPECKCL_B200_BANDS")) {
+    const int n = std::atoi(fb);
+    if (n > 0) nb = std::min(n, tile_rows);
+  }
+  return std::max(1, nb);
+}
 
 // Host pointers: the reference's filter_sub_image uploads the inputs and
 // downloads the results around its kernels (nlsar/conversion.cpp:22-142).
@@ -606,17 +616,7 @@ static int run_host_banded(const Plan& pl0, const float* const* hin, int nin, fl
   pl.P.K = K;
   const SceneGeom g = scene_geom(pl, H, W);
   if ((long long)g.tiles_x * g.tiles_y > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "scene too large");
-  int sms = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
-  const long long tiles = (long long)g.tiles_x * g.tiles_y;
-  int nb = (int)std::max(1LL, std::min<long long>(std::min(kMaxBands, g.tiles_y),
-                                                  tiles / ((long long)kBandWaves * sms)));
-  // DESPECKCL_B200_BANDS=n forces n bands (at most one per tile row): the
-  // tests use it to cut small scenes
-  if (const char* fb = std::getenv("DESPECKCL_B200_BANDS")) {
-    const int n = std::atoi(fb);
-    if (n > 0) nb = std::min(n, g.tiles_y);
-  }
+  const int nb = band_count(dev, (long long)g.tiles_x * g.tiles_y, g.tiles_y);
   HostPipe* hp = nullptr;
   rc = host_pipe(dev, 2 * (size_t)nb + 2, hp);
   if (rc) return rc;

@@ -46,6 +46,16 @@ int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scene
                  int variant = 0);
 // whether the call is served by the specialised kernel (variants apply)
 bool uses_specialised_kernel(const Plan& pl);
+// Copy streams and events of host-pointer calls (per thread and device):
+// `ev` holds at least the number of events asked for.
+struct HostPipe {
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> ev;
+};
+int host_pipe(int dev, size_t nev, HostPipe*& out);
+// Row bands of a host-pointer call over `tiles` tiles in `tile_rows` rows
+// (DESPECKCL_B200_BANDS overrides).
+int band_count(int dev, long long tiles, int tile_rows);
 // NL-SAR of a 3x3 covariance scene [18][H][W] (nlsar_dim3.cu): device
 // pointers on `st`, or host pointers (copied in and out, synchronous)
 int nlsar_covmat3_device(const Plan& pl, const float* cin, float* cout, int H, int W, cudaStream_t st);

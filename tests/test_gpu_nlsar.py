@@ -492,23 +492,31 @@ def test_covariance_3x3_path_matches_oracle(oracle, mode, sws, patches):
         assert ok_g >= 0.98
 
 
-def test_covariance_3x3_device_entry_point_equals_host(oracle):
+@pytest.mark.parametrize("shape,sws,patches,scales,bands", [
+    ((37, 29), 11, [3, 5], [1], None),          # generic kernel, one band
+    ((150, 47), 11, [3, 5], [1, 3], 5),         # generic kernel, host call in 5 row bands
+    ((170, 53), 21, [3, 5, 7], [1, 3], 4),      # specialised kernel, 4 bands
+])
+def test_covariance_3x3_device_entry_point_equals_host(oracle, monkeypatch, shape, sws, patches, scales, bands):
+    if bands is not None:
+        monkeypatch.setenv("DESPECKCL_B200_BANDS", str(bands))
+    H, W = shape
     tp, _ = _polsar_scene(32, 32, 43, homogeneous=True)
-    stats = oracle.training_covmat(tp, [3, 5], [1])
-    planes, cplx = _polsar_scene(37, 29, 44)
-    host = dcl.nlsar(cplx, 11, [3, 5], [1], stats, select_mode="argmax_enl")
+    stats = oracle.training_covmat(tp, [3, 5, 7], [1, 3])
+    planes, cplx = _polsar_scene(H, W, 44)
+    host = dcl.nlsar(cplx, sws, patches, scales, stats, select_mode="argmax_enl")
     hi = np.empty_like(planes)
-    hi[0::2] = host.real.reshape(9, 37, 29)
-    hi[1::2] = host.imag.reshape(9, 37, 29)
+    hi[0::2] = host.real.reshape(9, H, W)
+    hi[1::2] = host.imag.reshape(9, H, W)
     t = torch.from_numpy(planes).cuda()
     out = torch.empty_like(t)
     import ctypes
 
     import despeckcl_b200.api as api
-    pk, pp, npn = api._ints([3, 5])
-    sk, sp, nsn = api._ints([1])
+    pk, pp, npn = api._ints(patches)
+    sk, sp, nsn = api._ints(scales)
     arr, n, keep = api._entries(stats)
-    api._check(dcl.lib().dcl_nlsar_covmat_device(api._dptr(t), api._dptr(out), 37, 29, 3, 11, pp, npn, sp, nsn, arr,
+    api._check(dcl.lib().dcl_nlsar_covmat_device(api._dptr(t), api._dptr(out), H, W, 3, sws, pp, npn, sp, nsn, arr,
                                                  n, ctypes.c_float(15.0), ctypes.c_float(49.0), 1,
                                                  api._stream(None)))
     torch.cuda.synchronize()
