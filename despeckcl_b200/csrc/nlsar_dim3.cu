@@ -404,7 +404,7 @@ struct Fast3 {
   static constexpr int PHM = PH2 >= 0 ? PH2 : (PH1 >= 0 ? PH1 : PH0);
   static constexpr int TH = kT3H, TW = kT3W;
   static constexpr int THREADS = 2 * 32 * TH;  // two groups of one warp per row
-  static constexpr int K = 3;                  // offsets per batch along a window row
+  static constexpr int K = 7;                  // offsets per batch along a window row
   static constexpr int NA = 14;                // accumulators per patch size (group 1 uses 9)
   static constexpr int RS = TW + 2 * (PHM + WSH), RSH = TH + 2 * (PHM + WSH);
   static constexpr int RN = RS * RSH;
