@@ -154,8 +154,9 @@ __host__ __device__ inline FastStage fast_stage(int wsh, int phm, int tile_h) {
 }
 
 // The compile-time specialised kernel (nlsar_fast.cu) for the common
-// configurations; fast_kernel_supported() tells whether `F` has one.
-bool fast_kernel_supported(const FilterParams& F);
+// configurations; fast_kernel_supported() tells whether `F` has one (for
+// 8-plane covariance input when `full8`).
+bool fast_kernel_supported(const FilterParams& F, bool full8);
 // CTAs of the specialised kernel that gave up waiting for a staging copy
 // since the last call (the count is reset); 0 on success, -1 on a CUDA error
 int take_stage_timeouts(int* count);

@@ -36,58 +36,64 @@ namespace dcl {
 
 namespace {
 
-constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-template <int WSH, int PH0, int PH1, int PH2, int PX_, int TH_, bool FULL8_>
-struct Fast {
-  static constexpr int NP = (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
-  static constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
+// Shared-memory layout and launch shape of one instantiation: staging halo
+// PHX_ (the call's largest patch half), at most NPX_ patch sizes per pass,
+// PX_ vertically adjacent pixels per thread, TH_ tile rows.
+template <int WSH_, int PHX_, int NPX_, int PX_, int TH_, bool FULL8_>
+struct FastL {
+  static constexpr int WSH = WSH_, PHX = PHX_, NPX = NPX_;
   static constexpr int SWS = 2 * WSH + 1;
   static constexpr bool FULL8 = FULL8_;              // 8-plane covariance input and output
   static constexpr int TH = TH_, TW = 32, PX = PX_;  // tile rows; vertically adjacent pixels per thread
   static constexpr int WARPS = TH / PX, THREADS = 32 * WARPS;
-  // offsets per batch (SWS % K == 0): a single patch size leaves shared
-  // memory for seven, which amortises phase A's centre loads and the barriers
-  static constexpr int K = NP == 1 ? 7 : 3;
+  // offsets per batch (SWS % K == 0): single-patch passes with a small halo
+  // leave shared memory for seven, which amortises phase A's centre loads and
+  // the barriers
+  static constexpr int K = (NPX == 1 && PHX <= 3) ? 7 : 3;
   static constexpr int NA = FULL8 ? 12 : 8;          // accumulators per (pixel, patch size)
   static constexpr int NM = FULL8 ? 8 : 4;           // weighted sums kept for the selected combination
-  static constexpr int RS = TW + 2 * (PHM + WSH);    // scaled covariance region: RS x RSH
-  static constexpr int RSH = TH + 2 * (PHM + WSH);
+  static constexpr int RS = TW + 2 * (PHX + WSH);    // scaled covariance region: RS x RSH
+  static constexpr int RSH = TH + 2 * (PHX + WSH);
   static constexpr int RO = TW + 2 * WSH;            // original covariance region: RO x ROH
   static constexpr int ROH = TH + 2 * WSH;
-  static constexpr int SIMW = TW + 2 * PHM;          // similarity region: SIMW x SIMH
-  static constexpr int SIMH = TH + 2 * PHM;
-  // similarity row pitch, a multiple of 8 words: phase A's lanes write
-  // consecutive words; phase B reads 16-byte vectors, a quarter warp covering
-  // 8 consecutive segments of one row (contiguous, conflict free)
-  static constexpr int SIMP = (SIMW + 7) / 8 * 8;
-  static constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
-  static constexpr int HP = TW;                     // horizontal-sum row pitch (words), unpadded
-  static constexpr int HPL = K * SIMH * HP;         // one patch size's horizontal-sum plane
-  static constexpr int LUTREP = 16;                 // interleaved LUT copies: two lanes per copy
-  // shared memory, in 4-byte words
-  // the two TMA destinations start on 128-byte boundaries
-  // the TMA destinations start on 128-byte boundaries
+  // similarity region of the widest pass, SIMWX x SIMHX; its row pitch is a
+  // multiple of 8 words: phase A's lanes write consecutive words, phase B
+  // reads 16-byte vectors, a quarter warp covering 8 consecutive segments of
+  // one row (contiguous, conflict free)
+  static constexpr int SIMWX = TW + 2 * PHX, SIMHX = TH + 2 * PHX;
+  static constexpr int SIMPX = (SIMWX + 7) / 8 * 8;
+  static constexpr int HP = TW;                      // horizontal-sum row pitch (words), unpadded
+  static constexpr int HPL = K * SIMHX * HP;         // one patch size's horizontal-sum plane
+  // shared memory, in 4-byte words; the TMA destinations start on 128-byte
+  // boundaries
   static constexpr int OFF_CS = 0;
   static constexpr int OFF_CO = (OFF_CS + 4 * RS * RSH + 31) / 32 * 32;
   static constexpr int OFF_CO2 = (OFF_CO + 4 * RO * ROH + 31) / 32 * 32;  // 8-plane input only
   static constexpr int OFF_H = OFF_CO2 + (FULL8 ? 4 * RO * ROH : 0);
-  static constexpr int OFF_LD = OFF_H + NP * HPL;
+  static constexpr int OFF_LD = OFF_H + NPX * HPL;
   static constexpr int OFF_SIM = OFF_LD + RS * RSH;
-  static constexpr int OFF_LUT = OFF_SIM + K * SIMH * SIMP;
-  static constexpr int OFF_BAR = (OFF_LUT + NP * kMaxLut * LUTREP + 1) / 2 * 2;  // the mbarrier (8 bytes)
+  static constexpr int OFF_LUT = OFF_SIM + K * SIMHX * SIMPX;
+  // interleaved copies of the composite weight tables: 16 (two lanes per
+  // copy) where they fit, else 8 (four lanes per copy)
+  static constexpr int LUTREP = (OFF_LUT + NPX * kMaxLut * 16 + 4) * 4 <= 227 * 1024 ? 16 : 8;
+  static constexpr int OFF_BAR = (OFF_LUT + NPX * kMaxLut * LUTREP + 1) / 2 * 2;  // the mbarrier (8 bytes)
   static constexpr int WORDS = OFF_BAR + 2;
   static constexpr uint32_t CO_BYTES = 16u * RO * ROH;  // one TMA box each
   static constexpr uint32_t CS_BYTES = 16u * RS * RSH;
   static_assert(SWS % K == 0, "offset batches must tile a window row");
-  static_assert(PH0 >= 0, "at least one patch");
   static_assert(PX % 2 == 0, "pixels are accumulated in pairs");
-  static_assert(SIMP % 8 == 0 && SIMP >= 4 * 7 + 4 * NQ4, "phase-B segments must stay inside a row");
   static_assert(HP >= TW && HP % 4 == 0, "horizontal-sum pitch");
   static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
   static_assert(4 * RS <= 256 && 4 * RO <= 256 && RSH <= 256, "TMA box sides are at most 256 elements");
   static_assert(TH % PX == 0 && TH % 4 == 0, "tile rows");
 };
+
+template <int PH0, int PH1, int PH2>
+__host__ __device__ constexpr int np_of() {
+  return (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
+}
 
 // ---- TMA staging through one mbarrier --------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -165,27 +171,290 @@ __device__ __forceinline__ constexpr int ph_of(int j) {
   return j == 0 ? PH0 : (j == 1 ? PH1 : PH2);
 }
 
-template <int WSH, int PH0, int PH1, int PH2, int PX_, int TH_, bool FULL8_>
-__global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::THREADS, 1)
-    nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
-  using C = Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>;
-  constexpr int NP = C::NP, PHM = C::PHM, K = C::K, RS = C::RS, RSH = C::RSH, RO = C::RO;
-  constexpr int SIMW = C::SIMW, SIMH = C::SIMH, SIMP = C::SIMP, TW = C::TW, PX = C::PX;
-  constexpr int NT = C::THREADS, NW = C::WARPS, NA = C::NA, NM = C::NM;
-  constexpr bool FULL8 = C::FULL8;
-  extern __shared__ __align__(128) float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::OFF_BAR);
-  float4* sCs = reinterpret_cast<float4*>(smem + C::OFF_CS);
-  float4* sCo = reinterpret_cast<float4*>(smem + C::OFF_CO);
-  float4* sCo2 = reinterpret_cast<float4*>(smem + C::OFF_CO2);  // 8-plane input only
-  float* sH = smem + C::OFF_H;  // [NP][K][SIMH][HP]
-  float* sLd = smem + C::OFF_LD;
-  float* sSim = smem + C::OFF_SIM;
-  float* sLut = smem + C::OFF_LUT;
+// Selection state of a thread's PX pixels, kept across the passes.
+template <int PX, int NM>
+struct Best {
+  float e[PX], a[PX], s0[PX], m[PX][NM];
+  int rank[PX], combo[PX];
+};
+
+// One pass (one scale, the patch halves PH0 < PH1 < PH2 of this pass, -1
+// where unused) over all search-window offsets, on the staged tile; its
+// combinations update the selection state.  The staged scaled covariance
+// carries the halo of the call's largest patch; a pass with smaller patches
+// reads its region CO pixels further in.
+template <class L, int PH0, int PH1, int PH2>
+__device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParams& pp, float* smem,
+                                          Best<L::PX, L::NM>& best) {
+  constexpr int WSH = L::WSH, K = L::K, RS = L::RS, RO = L::RO, TW = L::TW, PX = L::PX;
+  constexpr int NT = L::THREADS, NW = L::WARPS, NA = L::NA, NM = L::NM;
+  constexpr bool FULL8 = L::FULL8;
+  constexpr int NP = np_of<PH0, PH1, PH2>();
+  constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
+  constexpr int CO = L::PHX - PHM;
+  constexpr int SIMW = TW + 2 * PHM, SIMH = L::TH + 2 * PHM;  // this pass's similarity region
+  constexpr int SIMP = (SIMW + 7) / 8 * 8;
+  constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
+  static_assert(PH0 >= 0 && NP <= L::NPX && CO >= 0, "pass shape");
+  static_assert(SIMP >= 4 * 7 + 4 * NQ4 && SIMP <= L::SIMPX, "phase-B segments must stay inside a row");
+  const float4* sCs = reinterpret_cast<const float4*>(smem + L::OFF_CS);
+  const float4* sCo = reinterpret_cast<const float4*>(smem + L::OFF_CO);
+  const float4* sCo2 = reinterpret_cast<const float4*>(smem + L::OFF_CO2);  // 8-plane input only
+  float* sH = smem + L::OFF_H;  // [NP][K][SIMH][HP]
+  const float* sLd = smem + L::OFF_LD;
+  float* sSim = smem + L::OFF_SIM;
+  float* sLut = smem + L::OFF_LUT;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int y0 = warp * PX;
   const float c2d = P.c2d;
+
+  // composite weight tables, LUTREP interleaved copies
+  for (int i = tid; i < NP * kMaxLut * L::LUTREP; i += NT) {
+    const int j = i / (kMaxLut * L::LUTREP);
+    const int e = (i - j * kMaxLut * L::LUTREP) / L::LUTREP;
+    sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
+  }
+  float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const ComboParams& cp = P.combo[pp.combo[j]];
+    inv_span[j] = 1.0f / cp.span;
+    nbias[j] = -cp.dmin * inv_span[j];
+    lm1[j] = cp.lm1;
+    dmax[j] = cp.dmax;
+  }
+  // this lane's copy of the table of component j
+  const float* lut_j[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) lut_j[j] = sLut + j * kMaxLut * L::LUTREP + (lane & (L::LUTREP - 1));
+  float2 acc[PX / 2][NP][NA];  // .x: pixel 2i, .y: pixel 2i+1
+#pragma unroll
+  for (int i = 0; i < PX / 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
+#pragma unroll
+      for (int a = 0; a < NA; ++a) acc[i][j][a] = make_float2(0.f, 0.f);
+  __syncthreads();
+
+  for (int dy = -WSH; dy <= WSH; ++dy) {
+    for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
+      // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
+      // thread and consecutive pixels on consecutive lanes (conflict free)
+      // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
+      for (int it = tid; it < SIMH * SIMP; it += NT) {
+        const int r = it / SIMP;
+        const int c = it - r * SIMP;
+        if (c >= SIMW) continue;
+        const int ci = (r + WSH + CO) * RS + (c + WSH + CO);
+        const float4 a = sCs[ci];
+        const float la = sLd[ci];
+        const int ni = ci + dy * RS + dx0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
+      }
+      __syncthreads();
+      // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
+      // quad of rows x 8 column segments, each quarter warp one row, so its
+      // 16-byte loads and stores are contiguous.
+      {
+        constexpr int QUADS = (SIMH + 3) / 4;
+        const int r_off = lane >> 3;
+        const int seg = lane & 7;
+        for (int q = warp; q < K * QUADS; q += NW) {
+          const int k = q / QUADS;
+          const int r = (q - k * QUADS) * 4 + r_off;
+          if (r < SIMH) {
+            const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
+            float s[4 * NQ4];
+#pragma unroll
+            for (int q4 = 0; q4 < NQ4; ++q4) {
+              const float4 v = row[q4];
+              s[4 * q4] = v.x;
+              s[4 * q4 + 1] = v.y;
+              s[4 * q4 + 2] = v.z;
+              s[4 * q4 + 3] = v.w;
+            }
+            float hs[NP][4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              float h[3] = {0.f, 0.f, 0.f};
+              float ring = s[o + PHM];
+#pragma unroll
+              for (int j = 0; j < 3; ++j)
+                if (ph_of<PH0, PH1, PH2>(j) == 0) h[j] = ring;
+#pragma unroll
+              for (int b = 1; b <= PHM; ++b) {
+                ring += s[o + PHM - b] + s[o + PHM + b];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                  if (ph_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
+              }
+#pragma unroll
+              for (int j = 0; j < NP; ++j) hs[j][o] = h[j];
+            }
+#pragma unroll
+            for (int j = 0; j < NP; ++j)
+              *reinterpret_cast<float4*>(sH + j * L::HPL + (k * SIMH + r) * L::HP + 4 * seg) =
+                  make_float4(hs[j][0], hs[j][1], hs[j][2], hs[j][3]);
+          }
+        }
+      }
+      __syncthreads();
+      // ---- C: vertical sums, weights, accumulation
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int dx = dx0 + k;
+        float w[PX][NP];
+        // vertical windows: patch j needs rows y0+PHM-ph_j .. y0+PHM+PX-1+ph_j
+        float hv[NP][PX + 2 * PHM];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          const float* col = sH + j * L::HPL + (k * SIMH + y0 + PHM - ph_of<PH0, PH1, PH2>(j)) * L::HP + lane;
+#pragma unroll
+          for (int r = 0; r < PX + 2 * ph_of<PH0, PH1, PH2>(j); ++r) hv[j][r] = col[r * L::HP];
+        }
+        if (dy == 0 && dx == 0) {
+#pragma unroll
+          for (int i = 0; i < PX; ++i)
+#pragma unroll
+            for (int j = 0; j < NP; ++j) w[i][j] = 1.0f;
+        } else {
+#pragma unroll
+          for (int i = 0; i < PX; ++i) {
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+              // top-down sum of the 2ph+1 rows (the first term starts the sum:
+              // no similarity sum is -0, so this equals 0 + ... bit for bit)
+              float d = hv[j][i];
+#pragma unroll
+              for (int a = 1; a <= 2 * ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + a];
+              // index = (unsigned)((clamp(d) - dmin) / (dmax - dmin) * (L - 1)):
+              // a saturating FMA clamps (and maps NaN to 0), a round-toward-zero
+              // add of 2^23 truncates, and the float's low mantissa bits are the
+              // index; d > dmax has weight 0
+              const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
+              const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
+              const int idx = __float_as_int(t) - 0x4B000000;
+              const float lw = lut_j[j][idx * L::LUTREP];
+              w[i][j] = (d > dmax[j]) ? 0.0f : lw;
+            }
+          }
+        }
+        // two pixels per packed (f32x2) operation; each component is
+        // rounded exactly like the scalar add / multiply / fma
+#pragma unroll
+        for (int i = 0; i < PX; i += 2) {
+          const int oa = (y0 + i + WSH + dy) * RO + (lane + WSH + dx);
+          const float4 va = sCo[oa];
+          const float4 vb = sCo[oa + RO];
+          const float2 vx = make_float2(va.x, vb.x), vy = make_float2(va.y, vb.y);
+          const float2 vz = make_float2(va.z, vb.z), vw = make_float2(va.w, vb.w);
+          const float2 x2 = __fmul2_rn(vx, vx), y2 = __fmul2_rn(vy, vy);
+          float2 ex[4];
+          if (FULL8) {
+            const float4 ea = sCo2[oa];
+            const float4 eb = sCo2[oa + RO];
+            ex[0] = make_float2(ea.x, eb.x);
+            ex[1] = make_float2(ea.y, eb.y);
+            ex[2] = make_float2(ea.z, eb.z);
+            ex[3] = make_float2(ea.w, eb.w);
+          }
+#pragma unroll
+          for (int j = 0; j < NP; ++j) {
+            float2* A = acc[i / 2][j];
+            const float2 ww = make_float2(w[i][j], w[i + 1][j]);
+            A[0] = __fadd2_rn(A[0], ww);
+            A[1] = __ffma2_rn(ww, ww, A[1]);
+            A[2] = __ffma2_rn(ww, vx, A[2]);
+            A[3] = __ffma2_rn(ww, vy, A[3]);
+            A[4] = __ffma2_rn(ww, x2, A[4]);
+            A[5] = __ffma2_rn(ww, y2, A[5]);
+            A[6] = __ffma2_rn(ww, vz, A[6]);
+            A[7] = __ffma2_rn(ww, vw, A[7]);
+            if (FULL8) {
+#pragma unroll
+              for (int e = 0; e < 4; ++e) A[(8 + e) % NA] = __ffma2_rn(ww, ex[e], A[(8 + e) % NA]);
+            }
+          }
+        }
+      }
+      // no barrier here: the next batch's phase A writes only the
+      // similarity map, which every warp finished reading (phase B)
+      // before the barrier above; its barrier after phase A orders this
+      // phase C's reads of the horizontal sums before they are rewritten
+    }
+  }
+
+  // ---- statistics, alpha, ENL', selection
+#pragma unroll
+  for (int i = 0; i < PX; ++i) {
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      float A[NA];
+#pragma unroll
+      for (int a = 0; a < NA; ++a) A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
+      const float s0 = A[0], s1 = A[1], s2 = A[2], s3 = A[3], s4 = A[4], s5 = A[5], s6 = A[6], s7 = A[7];
+      const float enl = s0 * s0 / s1;
+      const float i0 = s2 / s0, i1 = s3 / s0;
+      const float v0 = s4 / s0 - i0 * i0, v1 = s5 / s0 - i1 * i1;
+      float alpha = 0.0f;
+      alpha = fmaxf(alpha, fmaxf(0.0f, (v0 - i0 * i0) / v0));
+      alpha = fmaxf(alpha, fmaxf(0.0f, (v1 - i1 * i1) / v1));
+      if (P.alpha_zero) alpha = 0.0f;
+      const float oma = 1.0f - alpha;
+      const float enb = enl / (oma * oma + (alpha * alpha + 2.0f * alpha * (1.0f - alpha) / s0) * enl);
+      const int combo = pp.combo[j];
+      const int rank = P.combo[combo].rank;
+      const bool take = (P.select_mode == 0) || (enb > best.e[i]) || (enb == best.e[i] && rank < best.rank[i]);
+      const bool take_fb = !take && best.combo[i] < 0 && combo == P.fallback_combo;
+      if (take) {
+        best.e[i] = enb;
+        best.rank[i] = rank;
+      }
+      if (take || take_fb) {
+        best.combo[i] = combo;
+        best.a[i] = alpha;
+        best.s0[i] = s0;
+        best.m[i][0] = s2;
+        best.m[i][1] = s3;
+        best.m[i][2] = s6;
+        best.m[i][3] = s7;
+#pragma unroll
+        for (int e = 4; e < NM; ++e) best.m[i][e] = A[(e + 4) % NA];
+      }
+    }
+  }
+}
+
+template <int PH0, int PH1, int PH2>
+__device__ __forceinline__ bool pass_is(const PassParams& pp) {
+  constexpr int NP = np_of<PH0, PH1, PH2>();
+  return pp.np == NP && pp.ph[0] == PH0 && (NP < 2 || pp.ph[1] == PH1) && (NP < 3 || pp.ph[2] == PH2);
+}
+
+// The kernel: passes of shape A (patch halves A0 < A1 < A2) and, where B0 >=
+// 0, of shape B, staged for the largest patch half PHX.
+template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_>
+struct FastK {
+  using L = FastL<WSH, PHX, cmax(np_of<A0, A1, A2>(), np_of<B0, B1, B2>()), PX_, TH_, FULL8_>;
+};
+
+template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_>
+__global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L::THREADS, 1)
+    nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
+  using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
+  constexpr int RS = L::RS, RSH = L::RSH, RO = L::RO, TW = L::TW, PX = L::PX;
+  constexpr int NT = L::THREADS, NM = L::NM;
+  constexpr bool FULL8 = L::FULL8;
+  extern __shared__ __align__(128) float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::OFF_BAR);
+  float4* sCs = reinterpret_cast<float4*>(smem + L::OFF_CS);
+  float4* sCo = reinterpret_cast<float4*>(smem + L::OFF_CO);
+  float4* sCo2 = reinterpret_cast<float4*>(smem + L::OFF_CO2);  // 8-plane input only
+  float* sLd = smem + L::OFF_LD;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int y0 = warp * PX;
   if (tid == 0) mbar_init(bar, 1);
   __syncthreads();
   uint32_t parity = 0;
@@ -199,37 +468,36 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::TH
     const SceneDesc& S = scenes[lo];
     const int lt = tile - S.tile_begin + S.tile_skip;
     const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
-    const int vy0 = ty * C::TH, vx0 = tx * TW;
+    const int vy0 = ty * L::TH, vx0 = tx * TW;
     const int G = P.G;
 
     // stage the original covariance (tile + search halo; both of its float4
     // planes for 8-plane input) and the first pass's scaled covariance (tile
-    // + patch and search halo) with TMA; the barrier orders every thread's
-    // reads of the previous tile before the copies overwrite shared memory
+    // + largest patch and search halo) with TMA; the barrier orders every
+    // thread's reads of the previous tile before the copies overwrite shared
+    // memory
     __syncthreads();
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(bar, (FULL8 ? 2 : 1) * C::CO_BYTES + C::CS_BYTES);
+      mbar_expect_tx(bar, (FULL8 ? 2 : 1) * L::CO_BYTES + L::CS_BYTES);
       tma_load_2d(sCo, &S.tm_co, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
       if (FULL8) tma_load_2d(sCo2, &S.tm_co2, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
-      tma_load_2d(sCs, &S.tm_cs[P.pass[0].scale_slot], 4 * (vx0 - PHM - WSH + G), vy0 - PHM - WSH + G, bar);
+      tma_load_2d(sCs, &S.tm_cs[P.pass[0].scale_slot], 4 * (vx0 - PHX - WSH + G), vy0 - PHX - WSH + G, bar);
     }
     if (!stage_wait(bar, parity)) return;
     parity ^= 1u;
     for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
 
-    float2 acc[PX / 2][NP][NA];  // .x: pixel 2i, .y: pixel 2i+1
-    float best_e[PX], best_a[PX], best_s0[PX], best_m[PX][NM];
-    int best_rank[PX], best_combo[PX];
+    Best<PX, NM> best;
 #pragma unroll
     for (int i = 0; i < PX; ++i) {
-      best_e[i] = -1.0f;
-      best_rank[i] = 0x7fffffff;
-      best_combo[i] = -1;
-      best_a[i] = 0.f;
-      best_s0[i] = 1.f;
+      best.e[i] = -1.0f;
+      best.rank[i] = 0x7fffffff;
+      best.combo[i] = -1;
+      best.a[i] = 0.f;
+      best.s0[i] = 1.f;
 #pragma unroll
-      for (int d = 0; d < NM; ++d) best_m[i][d] = 0.f;
+      for (int d = 0; d < NM; ++d) best.m[i][d] = 0.f;
     }
 
     int loaded_slot = P.pass[0].scale_slot;
@@ -239,228 +507,21 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::TH
       if (pp.scale_slot != loaded_slot) {
         if (tid == 0) {
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_expect_tx(bar, C::CS_BYTES);
-          tma_load_2d(sCs, &S.tm_cs[pp.scale_slot], 4 * (vx0 - PHM - WSH + G), vy0 - PHM - WSH + G, bar);
+          mbar_expect_tx(bar, L::CS_BYTES);
+          tma_load_2d(sCs, &S.tm_cs[pp.scale_slot], 4 * (vx0 - PHX - WSH + G), vy0 - PHX - WSH + G, bar);
         }
         if (!stage_wait(bar, parity)) return;
         parity ^= 1u;
         for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
         loaded_slot = pp.scale_slot;
       }
-      // composite weight tables, LUTREP interleaved copies
-      for (int i = tid; i < NP * kMaxLut * C::LUTREP; i += NT) {
-        const int j = i / (kMaxLut * C::LUTREP);
-        const int e = (i - j * kMaxLut * C::LUTREP) / C::LUTREP;
-        sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
-      }
-      float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
-#pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const ComboParams& cp = P.combo[pp.combo[j]];
-        inv_span[j] = 1.0f / cp.span;
-        nbias[j] = -cp.dmin * inv_span[j];
-        lm1[j] = cp.lm1;
-        dmax[j] = cp.dmax;
-      }
-      // this lane's copy of the table of component j
-      const float* lut_j[NP];
-#pragma unroll
-      for (int j = 0; j < NP; ++j) lut_j[j] = sLut + j * kMaxLut * C::LUTREP + (lane & (C::LUTREP - 1));
-#pragma unroll
-      for (int i = 0; i < PX / 2; ++i)
-#pragma unroll
-        for (int j = 0; j < NP; ++j)
-#pragma unroll
-          for (int a = 0; a < NA; ++a) acc[i][j][a] = make_float2(0.f, 0.f);
-      __syncthreads();
-
-      for (int dy = -WSH; dy <= WSH; ++dy) {
-        for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
-          // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
-          // thread and consecutive pixels on consecutive lanes (conflict free)
-          // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-          for (int it = tid; it < SIMH * SIMP; it += NT) {
-            const int r = it / SIMP;
-            const int c = it - r * SIMP;
-            if (c >= SIMW) continue;
-            const int ci = (r + WSH) * RS + (c + WSH);
-            const float4 a = sCs[ci];
-            const float la = sLd[ci];
-            const int ni = ci + dy * RS + dx0;
-#pragma unroll
-            for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
-          }
-          __syncthreads();
-          // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
-          // quad of rows x 8 column segments, each quarter warp one row, so its
-          // 16-byte loads and stores are contiguous.
-          {
-            constexpr int QUADS = (SIMH + 3) / 4;
-            const int r_off = lane >> 3;
-            const int seg = lane & 7;
-            for (int q = warp; q < K * QUADS; q += NW) {
-              const int k = q / QUADS;
-              const int r = (q - k * QUADS) * 4 + r_off;
-              if (r < SIMH) {
-                const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
-                float s[4 * C::NQ4];
-#pragma unroll
-                for (int q4 = 0; q4 < C::NQ4; ++q4) {
-                  const float4 v = row[q4];
-                  s[4 * q4] = v.x;
-                  s[4 * q4 + 1] = v.y;
-                  s[4 * q4 + 2] = v.z;
-                  s[4 * q4 + 3] = v.w;
-                }
-                float hs[NP][4];
-#pragma unroll
-                for (int o = 0; o < 4; ++o) {
-                  float h[3] = {0.f, 0.f, 0.f};
-                  float ring = s[o + PHM];
-#pragma unroll
-                  for (int j = 0; j < 3; ++j)
-                    if (ph_of<PH0, PH1, PH2>(j) == 0) h[j] = ring;
-#pragma unroll
-                  for (int b = 1; b <= PHM; ++b) {
-                    ring += s[o + PHM - b] + s[o + PHM + b];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                      if (ph_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
-                  }
-#pragma unroll
-                  for (int j = 0; j < NP; ++j) hs[j][o] = h[j];
-                }
-#pragma unroll
-                for (int j = 0; j < NP; ++j)
-                  *reinterpret_cast<float4*>(sH + j * C::HPL + (k * SIMH + r) * C::HP + 4 * seg) =
-                      make_float4(hs[j][0], hs[j][1], hs[j][2], hs[j][3]);
-              }
-            }
-          }
-          __syncthreads();
-          // ---- C: vertical sums, weights, accumulation
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int dx = dx0 + k;
-            float w[PX][NP];
-            // vertical windows: patch j needs rows y0+PHM-ph_of<PH0, PH1, PH2>(j) .. y0+PHM+PX-1+ph_of<PH0, PH1, PH2>(j)
-            float hv[NP][PX + 2 * PHM];
-#pragma unroll
-            for (int j = 0; j < NP; ++j) {
-              const float* col = sH + j * C::HPL + (k * SIMH + y0 + PHM - ph_of<PH0, PH1, PH2>(j)) * C::HP + lane;
-#pragma unroll
-              for (int r = 0; r < PX + 2 * ph_of<PH0, PH1, PH2>(j); ++r) hv[j][r] = col[r * C::HP];
-            }
-            if (dy == 0 && dx == 0) {
-#pragma unroll
-              for (int i = 0; i < PX; ++i)
-#pragma unroll
-                for (int j = 0; j < NP; ++j) w[i][j] = 1.0f;
-            } else {
-#pragma unroll
-              for (int i = 0; i < PX; ++i) {
-#pragma unroll
-                for (int j = 0; j < NP; ++j) {
-                  // top-down sum of the 2ph+1 rows (the first term starts the sum:
-                  // no similarity sum is -0, so this equals 0 + ... bit for bit)
-                  float d = hv[j][i];
-#pragma unroll
-                  for (int a = 1; a <= 2 * ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + a];
-                  // index = (unsigned)((clamp(d) - dmin) / (dmax - dmin) * (L - 1)):
-                  // a saturating FMA clamps (and maps NaN to 0), a round-toward-zero
-                  // add of 2^23 truncates, and the float's low mantissa bits are the
-                  // index; d > dmax has weight 0
-                  const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
-                  const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
-                  const int idx = __float_as_int(t) - 0x4B000000;
-                  const float lw = lut_j[j][idx * C::LUTREP];
-                  w[i][j] = (d > dmax[j]) ? 0.0f : lw;
-                }
-              }
-            }
-            // two pixels per packed (f32x2) operation; each component is
-            // rounded exactly like the scalar add / multiply / fma
-#pragma unroll
-            for (int i = 0; i < PX; i += 2) {
-              const int oa = (y0 + i + WSH + dy) * RO + (lane + WSH + dx);
-              const float4 va = sCo[oa];
-              const float4 vb = sCo[oa + RO];
-              const float2 vx = make_float2(va.x, vb.x), vy = make_float2(va.y, vb.y);
-              const float2 vz = make_float2(va.z, vb.z), vw = make_float2(va.w, vb.w);
-              const float2 x2 = __fmul2_rn(vx, vx), y2 = __fmul2_rn(vy, vy);
-              float2 ex[4];
-              if (FULL8) {
-                const float4 ea = sCo2[oa];
-                const float4 eb = sCo2[oa + RO];
-                ex[0] = make_float2(ea.x, eb.x);
-                ex[1] = make_float2(ea.y, eb.y);
-                ex[2] = make_float2(ea.z, eb.z);
-                ex[3] = make_float2(ea.w, eb.w);
-              }
-#pragma unroll
-              for (int j = 0; j < NP; ++j) {
-                float2* A = acc[i / 2][j];
-                const float2 ww = make_float2(w[i][j], w[i + 1][j]);
-                A[0] = __fadd2_rn(A[0], ww);
-                A[1] = __ffma2_rn(ww, ww, A[1]);
-                A[2] = __ffma2_rn(ww, vx, A[2]);
-                A[3] = __ffma2_rn(ww, vy, A[3]);
-                A[4] = __ffma2_rn(ww, x2, A[4]);
-                A[5] = __ffma2_rn(ww, y2, A[5]);
-                A[6] = __ffma2_rn(ww, vz, A[6]);
-                A[7] = __ffma2_rn(ww, vw, A[7]);
-                if (FULL8) {
-#pragma unroll
-                  for (int e = 0; e < 4; ++e) A[(8 + e) % NA] = __ffma2_rn(ww, ex[e], A[(8 + e) % NA]);
-                }
-              }
-            }
-          }
-          // no barrier here: the next batch's phase A writes only the
-          // similarity map, which every warp finished reading (phase B)
-          // before the barrier above; its barrier after phase A orders this
-          // phase C's reads of the horizontal sums before they are rewritten
-        }
-      }
-
-      // ---- statistics, alpha, ENL', selection
-#pragma unroll
-      for (int i = 0; i < PX; ++i) {
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-          float A[NA];
-#pragma unroll
-          for (int a = 0; a < NA; ++a) A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
-          const float s0 = A[0], s1 = A[1], s2 = A[2], s3 = A[3], s4 = A[4], s5 = A[5], s6 = A[6], s7 = A[7];
-          const float enl = s0 * s0 / s1;
-          const float i0 = s2 / s0, i1 = s3 / s0;
-          const float v0 = s4 / s0 - i0 * i0, v1 = s5 / s0 - i1 * i1;
-          float alpha = 0.0f;
-          alpha = fmaxf(alpha, fmaxf(0.0f, (v0 - i0 * i0) / v0));
-          alpha = fmaxf(alpha, fmaxf(0.0f, (v1 - i1 * i1) / v1));
-          if (P.alpha_zero) alpha = 0.0f;
-          const float oma = 1.0f - alpha;
-          const float enb = enl / (oma * oma + (alpha * alpha + 2.0f * alpha * (1.0f - alpha) / s0) * enl);
-          const int combo = pp.combo[j];
-          const int rank = P.combo[combo].rank;
-          const bool take = (P.select_mode == 0) || (enb > best_e[i]) || (enb == best_e[i] && rank < best_rank[i]);
-          const bool take_fb = !take && best_combo[i] < 0 && combo == P.fallback_combo;
-          if (take) {
-            best_e[i] = enb;
-            best_rank[i] = rank;
-          }
-          if (take || take_fb) {
-            best_combo[i] = combo;
-            best_a[i] = alpha;
-            best_s0[i] = s0;
-            best_m[i][0] = s2;
-            best_m[i][1] = s3;
-            best_m[i][2] = s6;
-            best_m[i][3] = s7;
-#pragma unroll
-            for (int e = 4; e < NM; ++e) best_m[i][e] = A[(e + 4) % NA];
-          }
-        }
+      if constexpr (B0 < 0) {
+        fast_pass<L, A0, A1, A2>(P, pp, smem, best);
+      } else {
+        if (pass_is<A0, A1, A2>(pp))
+          fast_pass<L, A0, A1, A2>(P, pp, smem, best);
+        else
+          fast_pass<L, B0, B1, B2>(P, pp, smem, best);
       }
     }
 
@@ -475,12 +536,12 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::TH
       if (oy < 0 || ox < 0) continue;
       const int ci = (y + WSH) * RO + (lane + WSH);
       const float4 c = sCo[ci];
-      const float alpha = best_a[i], s0 = best_s0[i];
+      const float alpha = best.a[i], s0 = best.s0[i];
       const float oma = 1.0f - alpha;
-      const float c00 = oma * best_m[i][0] / s0 + alpha * c.x;
-      const float c11 = oma * best_m[i][1] / s0 + alpha * c.y;
-      const float cre = oma * best_m[i][2] / s0 + alpha * c.z;
-      const float cim = oma * best_m[i][3] / s0 + alpha * c.w;
+      const float c00 = oma * best.m[i][0] / s0 + alpha * c.x;
+      const float c11 = oma * best.m[i][1] / s0 + alpha * c.y;
+      const float cre = oma * best.m[i][2] / s0 + alpha * c.z;
+      const float cim = oma * best.m[i][3] / s0 + alpha * c.w;
       const size_t o = (size_t)oy * S.W + ox;
       if (FULL8) {
         // planes {Re, Im} of C00, C01, C10, C11; the second staged float4 is
@@ -488,13 +549,13 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::TH
         const float4 c2 = sCo2[ci];
         const size_t n = (size_t)S.H * S.W;
         S.cov_out[o] = c00;
-        S.cov_out[n + o] = oma * best_m[i][4 % NM] / s0 + alpha * c2.x;
+        S.cov_out[n + o] = oma * best.m[i][4 % NM] / s0 + alpha * c2.x;
         S.cov_out[2 * n + o] = cre;
         S.cov_out[3 * n + o] = cim;
-        S.cov_out[4 * n + o] = oma * best_m[i][5 % NM] / s0 + alpha * c2.y;
-        S.cov_out[5 * n + o] = oma * best_m[i][6 % NM] / s0 + alpha * c2.z;
+        S.cov_out[4 * n + o] = oma * best.m[i][5 % NM] / s0 + alpha * c2.y;
+        S.cov_out[5 * n + o] = oma * best.m[i][6 % NM] / s0 + alpha * c2.z;
         S.cov_out[6 * n + o] = c11;
-        S.cov_out[7 * n + o] = oma * best_m[i][7 % NM] / s0 + alpha * c2.w;
+        S.cov_out[7 * n + o] = oma * best.m[i][7 % NM] / s0 + alpha * c2.w;
       } else {
         const float am = sqrtf(c00), as = sqrtf(c11);
         const float r = 0.5f * (am + as);
@@ -502,31 +563,56 @@ __global__ void __launch_bounds__(Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>::TH
         S.phase[o] = atan2f(cim, cre);
         S.coh[o] = sqrtf(cim * cim + cre * cre) / (am * as);
       }
-      if (S.sel_out) S.sel_out[o] = best_combo[i];
+      if (S.sel_out) S.sel_out[o] = best.combo[i];
     }
   }
 }
 
-template <int WSH, int PH0, int PH1, int PH2, int PX_, int TH_, bool FULL8_>
+template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_>
 cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
-  using C = Fast<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>;
-  const size_t smem = (size_t)C::WORDS * 4;
+  using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
+  const size_t smem = (size_t)L::WORDS * 4;
   static size_t allowed[kMaxDevices];
-  const cudaError_t e =
-      allow_dynamic_smem((const void*)nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_>, smem, allowed);
+  const void* fn = (const void*)nlsar_fast_kernel<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>;
+  const cudaError_t e = allow_dynamic_smem(fn, smem, allowed);
   if (e != cudaSuccess) return e;
-  nlsar_fast_kernel<WSH, PH0, PH1, PH2, PX_, TH_, FULL8_><<<grid, C::THREADS, smem, st>>>(F, d_scenes);
+  nlsar_fast_kernel<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_><<<grid, L::THREADS, smem, st>>>(F, d_scenes);
   return cudaGetLastError();
 }
 
-template <int PX_, int TH_, bool FULL8_>
-cudaError_t launch_fast_px(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
-  const PassParams& p0 = F.pass[0];
-  if (p0.np == 3) return launch_fast_t<10, 1, 2, 3, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
-  switch (p0.ph[0]) {
-    case 1: return launch_fast_t<10, 1, -1, -1, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
-    case 2: return launch_fast_t<10, 2, -1, -1, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
-    default: return launch_fast_t<10, 3, -1, -1, PX_, TH_, FULL8_>(F, d_scenes, grid, st);
+// pass shapes of a call: 1 every pass {1,2,3}; 2..6 every pass the single
+// half 1..5; 7 every pass {1,2,3} or {4,5} with at least one {4,5} (patches
+// 3..11 at each scale); 0 none of these
+int fast_shape(const FilterParams& F, bool full8) {
+  if (F.wsh != 10 || F.npass < 1) return 0;
+  auto is = [](const PassParams& p, int n, int a0, int a1, int a2) {
+    return p.np == n && p.ph[0] == a0 && (n < 2 || p.ph[1] == a1) && (n < 3 || p.ph[2] == a2);
+  };
+  bool all123 = true, all45_or_123 = true, any45 = false, single = true;
+  const int h0 = F.pass[0].ph[0];
+  for (int i = 0; i < F.npass; ++i) {
+    const PassParams& p = F.pass[i];
+    const bool s123 = is(p, 3, 1, 2, 3), s45 = is(p, 2, 4, 5, -1);
+    all123 = all123 && s123;
+    all45_or_123 = all45_or_123 && (s123 || s45);
+    any45 = any45 || s45;
+    single = single && p.np == 1 && p.ph[0] == h0;
+  }
+  if (all123) return 1;
+  if (single && h0 >= 1 && h0 <= (full8 ? 3 : 5)) return 1 + h0;
+  if (!full8 && all45_or_123 && any45) return 7;
+  return 0;
+}
+
+template <int PX_>
+cudaError_t launch_fast_insar(int shape, const FilterParams& F, const SceneDesc* d_scenes, int grid,
+                              cudaStream_t st) {
+  constexpr int T = kFastTileH;
+  switch (shape) {
+    case 1: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, PX_, T, false>(F, d_scenes, grid, st);
+    case 2: return launch_fast_t<10, 1, 1, -1, -1, -1, -1, -1, PX_, T, false>(F, d_scenes, grid, st);
+    case 3: return launch_fast_t<10, 2, 2, -1, -1, -1, -1, -1, PX_, T, false>(F, d_scenes, grid, st);
+    default: return launch_fast_t<10, 3, 3, -1, -1, -1, -1, -1, PX_, T, false>(F, d_scenes, grid, st);
   }
 }
 
@@ -546,32 +632,38 @@ int take_stage_timeouts(int* count) {
 }
 
 // Specialisations available: the search window 21 (half 10) with every pass
-// holding the patch halves {1,2,3} (patches 3,5,7) or the single half 1, 2 or
-// 3 (reference mode).  Returns false when no specialisation matches.
-bool fast_kernel_supported(const FilterParams& F) {
-  if (F.wsh != 10 || F.npass < 1) return false;
-  const PassParams& p0 = F.pass[0];
-  for (int i = 0; i < F.npass; ++i) {
-    const PassParams& p = F.pass[i];
-    if (p.np != p0.np) return false;
-    for (int j = 0; j < p.np; ++j)
-      if (p.ph[j] != p0.ph[j]) return false;
-  }
-  if (p0.np == 3) return p0.ph[0] == 1 && p0.ph[1] == 2 && p0.ph[2] == 3;
-  if (p0.np == 1) return p0.ph[0] >= 1 && p0.ph[0] <= 3;
-  return false;
-}
+// holding the patch halves {1,2,3} (patches 3,5,7), or every pass one and the
+// same patch half (reference selection; halves 1..5 for InSAR input, 1..3 for
+// 8-plane input), or, for InSAR input, every pass {1,2,3} or {4,5} (patches
+// 3..11 at each scale, the reference example's settings).
+bool fast_kernel_supported(const FilterParams& F, bool full8) { return fast_shape(F, full8) != 0; }
 
 // InSAR input (32 x 32 tiles): variant 0 has 2 pixels per thread in
 // 512-thread CTAs (the default), variant 1 4 pixels per thread in 256-thread
-// CTAs; the batch autotuner times both.  8-plane covariance input: 32 x 24
-// tiles, 2 pixels per thread, 384-thread CTAs (the second staged covariance
-// plane and its four accumulators per patch size need the room).
+// CTAs (the patch sizes up to 7; the batch autotuner times both).  8-plane
+// covariance input: 32 x 24 tiles, 2 pixels per thread, 384-thread CTAs (the
+// second staged covariance plane and its four accumulators per patch size
+// need the room).
 cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
                               int variant, bool full8) {
-  if (full8) return launch_fast_px<2, kFastTileH8, true>(F, d_scenes, grid, st);
-  if (variant == 1) return launch_fast_px<4, kFastTileH, false>(F, d_scenes, grid, st);
-  return launch_fast_px<2, kFastTileH, false>(F, d_scenes, grid, st);
+  const int shape = fast_shape(F, full8);
+  constexpr int T8 = kFastTileH8, T = kFastTileH;
+  if (full8) {
+    switch (shape) {
+      case 1: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
+      case 2: return launch_fast_t<10, 1, 1, -1, -1, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
+      case 3: return launch_fast_t<10, 2, 2, -1, -1, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
+      default: return launch_fast_t<10, 3, 3, -1, -1, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
+    }
+  }
+  switch (shape) {
+    case 5: return launch_fast_t<10, 4, 4, -1, -1, -1, -1, -1, 2, T, false>(F, d_scenes, grid, st);
+    case 6: return launch_fast_t<10, 5, 5, -1, -1, -1, -1, -1, 2, T, false>(F, d_scenes, grid, st);
+    case 7: return launch_fast_t<10, 5, 1, 2, 3, 4, 5, -1, 2, T, false>(F, d_scenes, grid, st);
+    default:
+      if (variant == 1) return launch_fast_insar<4>(shape, F, d_scenes, grid, st);
+      return launch_fast_insar<2>(shape, F, d_scenes, grid, st);
+  }
 }
 
 }  // namespace dcl

@@ -231,7 +231,7 @@ int make_plan(int sws, const int* patches, int np, const int* scales, int ns, co
   F.G = F.wsh + F.phm + pl.shm;
   // the specialised kernel serves the common settings, in 32 x 32 tiles for
   // InSAR input and 32 x 24 tiles for 8-plane covariance input
-  pl.fast = !g_force_generic && fast_kernel_supported(F);
+  pl.fast = !g_force_generic && fast_kernel_supported(F, full8);
   if (pl.fast && full8) F.tile_h = kFastTileH8;
   return DCL_OK;
 }
@@ -457,7 +457,7 @@ int launch_fused(const Plan& pl, const FilterParams& F, const SceneDesc* d_scene
     cudaEventCreate(&b);
     cudaEventRecord(a, st);
   }
-  const bool fast = pl.fast && fast_kernel_supported(F);
+  const bool fast = pl.fast && fast_kernel_supported(F, pl.full8);
   const cudaError_t e = fast ? launch_nlsar_fast(F, d_scenes, F.total_tiles, st, variant, pl.full8)
                              : launch_nlsar_fused(pl.full8, F, d_scenes, smem, F.total_tiles, st);
   if (g_prof.on) {

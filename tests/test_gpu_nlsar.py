@@ -249,6 +249,41 @@ def test_covariance_specialised_and_generic_kernels_agree(tmp_path, oracle, trai
     assert (err <= 1e-4).mean() >= 0.99, err.max()
 
 
+@pytest.mark.parametrize("mode", ["argmax_enl", "reference"])
+def test_example_settings_specialised_and_generic_kernels_agree(tmp_path, mode):
+    # the reference example's settings (patches 3..11, scales 1..5): passes of
+    # {3,5,7} and {9,11} at each scale, staged for patch 11, in the
+    # specialised kernel; reference selection runs patch 11 at scale 5 alone.
+    # The generic kernel, forced in a child process, must agree up to FP32
+    # summation order.
+    import os
+    import pickle
+    import subprocess
+    import sys
+
+    P, S = [3, 5, 7, 9, 11], [1, 3, 5]
+    t1, t2, tp = synthetic.training_area(64, seed=3)
+    stats = dcl.nlsar_train_insar(t1, t2, tp, P, S)
+    a1, a2, ph = synthetic.insar_scene(70, 90, 32)
+    fast = run_gpu(a1, a2, ph, stats, mode, patches=P, scales=S)
+    f = tmp_path / "in.pkl"
+    st = {k: (v.lut_size, v.dissims_min, v.dissims_max, v.quantilles, v.chi2cdf_inv) for k, v in stats.items()}
+    pickle.dump((a1, a2, ph, st), open(f, "wb"))
+    code = (
+        "import pickle,sys,numpy as np; sys.path.insert(0, %r); import despeckcl_b200 as d; "
+        "a1,a2,ph,st=pickle.load(open(%r,'rb')); "
+        "st={k: d.Stats(*v) for k,v in st.items()}; "
+        "r=d.nlsar_insar(a1,a2,ph,21,%r,%r,st,select_mode=%r); "
+        "pickle.dump(r, open(%r,'wb'))" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), str(f),
+                                          P, S, mode, str(tmp_path / "out.pkl")))
+    env = dict(os.environ, DESPECKCL_B200_GENERIC="1")
+    subprocess.run([sys.executable, "-c", code], env=env, check=True)
+    gen = pickle.load(open(tmp_path / "out.pkl", "rb"))
+    e = np.abs(fast[0] - gen[0]) / gen[0]
+    assert (e <= 1e-4).mean() >= 0.99
+    assert (wrapped(fast[1] - gen[1]) <= 1e-3).mean() >= 0.99
+
+
 def test_host_entry_point_equals_device_entry_point(train_stats):
     a1, a2, ph = synthetic.insar_scene(70, 90, 10)
     host = dcl.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode="argmax_enl")
