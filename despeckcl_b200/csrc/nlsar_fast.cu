@@ -1,6 +1,8 @@
 // Fused NL-SAR tile kernel specialised at compile time on the search-window
-// half size and the patch half sizes of a pass (the common configurations),
-// for sm_100a.  Same semantics as the generic kernel in nlsar_kernels.cu.
+// half size and the patch half sizes of the passes (the common
+// configurations: one pass shape, or two such as {3,5,7} and {9,11} with the
+// tile staged for the largest patch), for sm_100a.  Same semantics as the
+// generic kernel in nlsar_kernels.cu.
 //
 // Per CTA: a 32 x 32 output tile (32 x 24 for 8-plane covariance input), each
 // thread owning 2 (16 warps) or 4 (8 warps) vertically consecutive pixels of
