@@ -7,7 +7,7 @@
 // Per CTA: a 32 x 32 output tile (32 x 24 for 8-plane covariance input), each
 // thread owning 2 (16 warps) or 4 (8 warps) vertically consecutive pixels of
 // one column.  For every scale the search-window offsets are taken three at a
-// time (seven when a pass has one patch size) along a row of the window (same
+// time (seven when every pass has one patch size of at most 7) along a row of the window (same
 // dy, consecutive dx, so a thread's neighbour loads overlap across the batch):
 //   A  GLR similarities of the batch on the tile plus the patch halo
 //      (each thread: one pixel x three offsets); the measure is evaluated in
