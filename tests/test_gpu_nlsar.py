@@ -249,19 +249,24 @@ def test_covariance_specialised_and_generic_kernels_agree(tmp_path, oracle, trai
     assert (err <= 1e-4).mean() >= 0.99, err.max()
 
 
-@pytest.mark.parametrize("mode", ["argmax_enl", "reference"])
-def test_example_settings_specialised_and_generic_kernels_agree(tmp_path, mode):
+@pytest.mark.parametrize("P,S,mode", [
+    ([3, 5, 7, 9, 11], [1, 3, 5], "argmax_enl"),
+    ([3, 5, 7, 9, 11], [1, 3, 5], "reference"),
+    ([9], [1, 3], "argmax_enl"),
+    ([9, 11], [1, 3], "argmax_enl"),
+])
+def test_example_settings_specialised_and_generic_kernels_agree(tmp_path, P, S, mode):
     # the reference example's settings (patches 3..11, scales 1..5): passes of
     # {3,5,7} and {9,11} at each scale, staged for patch 11, in the
     # specialised kernel; reference selection runs patch 11 at scale 5 alone.
-    # The generic kernel, forced in a child process, must agree up to FP32
-    # summation order.
+    # Patch 9 alone and passes of {9,11} alone take the other instantiations
+    # of those sizes.  The generic kernel, forced in a child process, must
+    # agree up to FP32 summation order.
     import os
     import pickle
     import subprocess
     import sys
 
-    P, S = [3, 5, 7, 9, 11], [1, 3, 5]
     t1, t2, tp = synthetic.training_area(64, seed=3)
     stats = dcl.nlsar_train_insar(t1, t2, tp, P, S)
     a1, a2, ph = synthetic.insar_scene(70, 90, 32)
