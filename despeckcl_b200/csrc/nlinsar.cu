@@ -15,7 +15,9 @@
 //      Kullback-Leibler divergence of the estimates (sim_measures.h) on the
 //      similarity grid -- with the two pixels swapped in the tile interior for
 //      the first wsh window rows, which the reference copies from the mirrored
-//      offset (precompute_similarities_{1st,2nd}_pass) --, p x p sums rows
+//      offset (precompute_similarities_{1st,2nd}_pass): each lower-row offset
+//      is taken with its mirror, whose interior maps are the lower offset's
+//      shifted, only its border evaluated --, p x p sums rows
 //      first (precompute_patch_similarities.cl), w = exp(S/h + KL/T) with
 //      NaN / inf -> 0 and the centre weight 0 (compute_weights.cl), the looks
 //      (sum w)^2 / sum w^2 accumulated in offset order
@@ -55,6 +57,8 @@ struct NlGeom {
   int ntx, nty;        // tiles per row / column
   int lmin;
   float h, T;
+  int nborder;         // similarity-grid positions outside the interior the reference copies
+  int mirror;          // 1: offsets of the lower window rows share their maps with their mirrors
 };
 
 __device__ __forceinline__ int clampn(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -126,53 +130,133 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int no = g.sws * g.sws, kc = g.wsh * g.sws + g.wsh;
   float* wt = wout + (size_t)blockIdx.x * no * npix;
   __syncthreads();
-  for (int hh = 0; hh < g.sws; ++hh)
-    for (int ww = 0; ww < g.sws; ++ww) {
-      const int k = hh * g.sws + ww;
-      for (int it = tid; it < nsim; it += kThreads) {
-        const int h = it / g.hsim, w = it - h * g.hsim;
-        const bool interior = h >= g.wsh && w >= g.wsh && w < g.hsim - g.wsh;
-        int c = (h + g.wsh) * kTile + (w + g.wsh), q = (h + hh) * kTile + (w + ww);
-        if (interior && hh < g.wsh) {
-          const int t = c;
-          c = q;
-          q = t;
-        }
-        sS[it] = pixel_sim(sA1[c], sA2[c], sDp[c], sA1[q], sA2[q], sDp[q]);
-        sK[it] = pixel_kl(sRf[c], sPf[c], sCf[c], sRf[q], sPf[q], sCf[q]);
+  // similarities and divergences of offset (hh, ww) on the whole grid, with
+  // the two pixels swapped in the interior for the first wsh window rows (the
+  // values the reference copies from the mirrored offset)
+  auto sims_direct = [&](int hh, int ww) {
+    for (int it = tid; it < nsim; it += kThreads) {
+      const int h = it / g.hsim, w = it - h * g.hsim;
+      const bool interior = h >= g.wsh && w >= g.wsh && w < g.hsim - g.wsh;
+      int c = (h + g.wsh) * kTile + (w + g.wsh), q = (h + hh) * kTile + (w + ww);
+      if (interior && hh < g.wsh) {
+        const int t = c;
+        c = q;
+        q = t;
       }
-      __syncthreads();
-      for (int it = tid; it < nrow; it += kThreads) {
-        const int r = it / g.hori, col = it - r * g.hori;
-        float rs = 0.0f, rk = 0.0f;
-        for (int ky = 0; ky < g.p; ++ky) {
-          rs += sS[r * g.hsim + col + ky];
-          rk += sK[r * g.hsim + col + ky];
-        }
-        sRS[it] = rs;
-        sRK[it] = rk;
+      sS[it] = pixel_sim(sA1[c], sA2[c], sDp[c], sA1[q], sA2[q], sDp[q]);
+      sK[it] = pixel_kl(sRf[c], sPf[c], sCf[c], sRf[q], sPf[q], sCf[q]);
+    }
+  };
+  // p-wide row sums of a map given by `val(h, w)` (similarity, divergence)
+  auto row_sums = [&](auto val) {
+    for (int it = tid; it < nrow; it += kThreads) {
+      const int r = it / g.hori, col = it - r * g.hori;
+      float rs = 0.0f, rk = 0.0f;
+      for (int ky = 0; ky < g.p; ++ky) {
+        const float2 v = val(r, col + ky);
+        rs += v.x;
+        rk += v.y;
       }
-      __syncthreads();
+      sRS[it] = rs;
+      sRK[it] = rk;
+    }
+  };
+  auto direct_val = [&](int h, int w) { return make_float2(sS[h * g.hsim + w], sK[h * g.hsim + w]); };
+  // p-wide column sums, weights and looks of offset k
+  auto weights_of = [&](int k) {
 #pragma unroll
-      for (int q = 0; q < kMaxPixPerThread; ++q) {
-        const int pix = tid + q * kThreads;
-        if (pix < npix) {
-          const int x = pix / g.hori, y = pix - x * g.hori;
-          float s = sRS[x * g.hori + y], kl = sRK[x * g.hori + y];
-          for (int kx = 1; kx < g.p; ++kx) {
-            s += sRS[(x + kx) * g.hori + y];
-            kl += sRK[(x + kx) * g.hori + y];
-          }
-          float wv = expf(s / g.h + kl / g.T);
-          if (isnan(wv) || isinf(wv)) wv = 0.0f;
-          if (k == kc) wv = 0.0f;
-          wt[(size_t)k * npix + pix] = wv;
-          s1[q] += wv;
-          s2[q] += wv * wv;
+    for (int q = 0; q < kMaxPixPerThread; ++q) {
+      const int pix = tid + q * kThreads;
+      if (pix < npix) {
+        const int x = pix / g.hori, y = pix - x * g.hori;
+        float s = sRS[x * g.hori + y], kl = sRK[x * g.hori + y];
+        for (int kx = 1; kx < g.p; ++kx) {
+          s += sRS[(x + kx) * g.hori + y];
+          kl += sRK[(x + kx) * g.hori + y];
         }
+        float wv = expf(s / g.h + kl / g.T);
+        if (isnan(wv) || isinf(wv)) wv = 0.0f;
+        if (k == kc) wv = 0.0f;
+        wt[(size_t)k * npix + pix] = wv;
+        s1[q] += wv;
+        s2[q] += wv * wv;
       }
+    }
+  };
+  if (!g.mirror) {
+    for (int hh = 0; hh < g.sws; ++hh)
+      for (int ww = 0; ww < g.sws; ++ww) {
+        sims_direct(hh, ww);
+        __syncthreads();
+        row_sums(direct_val);
+        __syncthreads();
+        weights_of(hh * g.sws + ww);
+        __syncthreads();
+      }
+  } else {
+    // the centre window row, computed as the reference computes it
+    for (int ww = 0; ww < g.sws; ++ww) {
+      sims_direct(g.wsh, ww);
+      __syncthreads();
+      row_sums(direct_val);
+      __syncthreads();
+      weights_of(g.wsh * g.sws + ww);
       __syncthreads();
     }
+    // every lower-row offset with its mirror: the mirror's interior values are
+    // the lower offset's maps shifted by the mirror's offset (the very values
+    // the reference copies), its border values are computed here
+    float* sBS = sRK + nrow;  // mirror's border: similarity, divergence
+    float* sBK = sBS + g.nborder;
+    const int top = g.wsh * g.hsim, band = 2 * g.wsh;
+    for (int hl = g.wsh + 1; hl < g.sws; ++hl)
+      for (int wl = 0; wl < g.sws; ++wl) {
+        const int hu = 2 * g.wsh - hl, wu = 2 * g.wsh - wl;
+        for (int it = tid; it < nsim + g.nborder; it += kThreads) {
+          int c, q;
+          if (it < nsim) {
+            const int h = it / g.hsim, w = it - h * g.hsim;
+            c = (h + g.wsh) * kTile + (w + g.wsh);
+            q = (h + hl) * kTile + (w + wl);
+            sS[it] = pixel_sim(sA1[c], sA2[c], sDp[c], sA1[q], sA2[q], sDp[q]);
+            sK[it] = pixel_kl(sRf[c], sPf[c], sCf[c], sRf[q], sPf[q], sCf[q]);
+          } else {
+            const int ib = it - nsim;
+            int h, w;
+            if (ib < top) {
+              h = ib / g.hsim;
+              w = ib - h * g.hsim;
+            } else {
+              const int j = ib - top;
+              h = g.wsh + j / band;
+              const int m = j - (j / band) * band;
+              w = m < g.wsh ? m : g.hsim - band + m;
+            }
+            c = (h + g.wsh) * kTile + (w + g.wsh);
+            q = (h + hu) * kTile + (w + wu);
+            sBS[ib] = pixel_sim(sA1[c], sA2[c], sDp[c], sA1[q], sA2[q], sDp[q]);
+            sBK[ib] = pixel_kl(sRf[c], sPf[c], sCf[c], sRf[q], sPf[q], sCf[q]);
+          }
+        }
+        __syncthreads();
+        row_sums(direct_val);
+        __syncthreads();
+        weights_of(hl * g.sws + wl);
+        __syncthreads();
+        const int dh = hu - g.wsh, dw = wu - g.wsh;
+        row_sums([&](int h, int w) {
+          if (h >= g.wsh && w >= g.wsh && w < g.hsim - g.wsh) {
+            const int i = (h + dh) * g.hsim + (w + dw);
+            return make_float2(sS[i], sK[i]);
+          }
+          const int ib = h < g.wsh ? h * g.hsim + w : top + (h - g.wsh) * band + (w < g.wsh ? w : w - g.hsim + band);
+          return make_float2(sBS[ib], sBK[ib]);
+        });
+        __syncthreads();
+        weights_of(hu * g.sws + wu);
+        __syncthreads();
+      }
+  }
 #pragma unroll
   for (int q = 0; q < kMaxPixPerThread; ++q) {
     const int pix = tid + q * kThreads;
@@ -325,7 +409,9 @@ __global__ void __launch_bounds__(kEstThreads)
 }
 
 size_t weights_smem(const NlGeom& g) {
-  return ((size_t)6 * kTile * kTile + 2 * (size_t)g.hsim * g.hsim + 2 * (size_t)g.hsim * g.hori) * sizeof(float);
+  return ((size_t)6 * kTile * kTile + 2 * (size_t)g.hsim * g.hsim + 2 * (size_t)g.hsim * g.hori +
+          (g.mirror ? 2 * (size_t)g.nborder : 0)) *
+         sizeof(float);
 }
 
 int nlinsar_geom(int H, int W, int sws, int p, int lmin, NlGeom& g) {
@@ -347,6 +433,11 @@ int nlinsar_geom(int H, int W, int sws, int p, int lmin, NlGeom& g) {
   g.ov = g.wsh + g.psh;
   g.hsim = kTile - sws + 1;
   g.hori = kTile - 2 * g.ov;
+  // mirrored maps need an interior (rows from wsh, columns wsh .. hsim-wsh-1)
+  // and room for the mirror's border values
+  g.nborder = g.wsh * g.hsim + (g.hsim - g.wsh) * 2 * g.wsh;
+  g.mirror = 2 * g.wsh < g.hsim ? 1 : 0;
+  if (g.mirror && weights_smem(g) > 227 * 1024) g.mirror = 0;
   if (g.hori < 1) return set_error(DCL_ERR_UNSUPPORTED, "search window and patch too large for the 80 x 80 tiles");
   if ((g.hori * g.hori + kThreads - 1) / kThreads > kMaxPixPerThread || weights_smem(g) > 227 * 1024)
     return set_error(DCL_ERR_UNSUPPORTED, "search window %d with patch %d: tile state exceeds shared memory", sws, p);
