@@ -700,7 +700,22 @@ cudaError_t launch3_fast_t(const FilterParams& F, const Scene3& S, unsigned tile
   return cudaGetLastError();
 }
 
-// the specialised 3x3 kernel for the plans fast_kernel_supported() accepts
+// whether the specialised 3x3 kernel has the call's pass shapes: every pass
+// the patch halves {1,2,3}, or every pass one and the same half 1..3
+bool fast3_supported(const FilterParams& F) {
+  if (F.wsh != 10 || F.npass < 1) return false;
+  const PassParams& p0 = F.pass[0];
+  for (int i = 0; i < F.npass; ++i) {
+    const PassParams& p = F.pass[i];
+    if (p.np != p0.np) return false;
+    for (int j = 0; j < p.np; ++j)
+      if (p.ph[j] != p0.ph[j]) return false;
+  }
+  if (p0.np == 3) return p0.ph[0] == 1 && p0.ph[1] == 2 && p0.ph[2] == 3;
+  return p0.np == 1 && p0.ph[0] >= 1 && p0.ph[0] <= 3;
+}
+
+// the specialised 3x3 kernel, for the plans fast3_supported() accepts
 cudaError_t launch3_fast(const FilterParams& F, const Scene3& S, unsigned tiles, cudaStream_t st) {
   const PassParams& p0 = F.pass[0];
   if (p0.np == 3) return launch3_fast_t<1, 2, 3>(F, S, tiles, st);
@@ -896,7 +911,7 @@ static int launch3_rows(const Run3& r, int t0, int t1, cudaStream_t st) {
   const unsigned tiles = (unsigned)((t1 - t0) * S.tiles_x);
   F.total_tiles = (int)tiles;
   cudaError_t e;
-  if (r.pl.fast) {
+  if (r.pl.fast && fast3_supported(F)) {
     e = launch3_fast(F, S, tiles, st);
   } else {
     static size_t allowed[kMaxDevices];

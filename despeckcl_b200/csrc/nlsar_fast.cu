@@ -584,7 +584,7 @@ cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int 
 
 // pass shapes of a call: 1 every pass {1,2,3}; 2..6 every pass the single
 // half 1..5; 7 every pass {1,2,3} or {4,5} with at least one {4,5} (patches
-// 3..11 at each scale); 0 none of these
+// 3..11 at each scale, InSAR and 8-plane input); 0 none of these
 int fast_shape(const FilterParams& F, bool full8) {
   if (F.wsh != 10 || F.npass < 1) return 0;
   auto is = [](const PassParams& p, int n, int a0, int a1, int a2) {
@@ -602,7 +602,7 @@ int fast_shape(const FilterParams& F, bool full8) {
   }
   if (all123) return 1;
   if (single && h0 >= 1 && h0 <= (full8 ? 3 : 5)) return 1 + h0;
-  if (!full8 && all45_or_123 && any45) return 7;
+  if (all45_or_123 && any45) return 7;
   return 0;
 }
 
@@ -636,8 +636,8 @@ int take_stage_timeouts(int* count) {
 // Specialisations available: the search window 21 (half 10) with every pass
 // holding the patch halves {1,2,3} (patches 3,5,7), or every pass one and the
 // same patch half (reference selection; halves 1..5 for InSAR input, 1..3 for
-// 8-plane input), or, for InSAR input, every pass {1,2,3} or {4,5} (patches
-// 3..11 at each scale, the reference example's settings).
+// 8-plane input), or every pass {1,2,3} or {4,5} (patches 3..11 at each
+// scale, the reference example's settings).
 bool fast_kernel_supported(const FilterParams& F, bool full8) { return fast_shape(F, full8) != 0; }
 
 // InSAR input (32 x 32 tiles): variant 0 has 2 pixels per thread in
@@ -655,6 +655,7 @@ cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, 
       case 1: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
       case 2: return launch_fast_t<10, 1, 1, -1, -1, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
       case 3: return launch_fast_t<10, 2, 2, -1, -1, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
+      case 7: return launch_fast_t<10, 5, 1, 2, 3, 4, 5, -1, 2, T8, true>(F, d_scenes, grid, st);
       default: return launch_fast_t<10, 3, 3, -1, -1, -1, -1, -1, 2, T8, true>(F, d_scenes, grid, st);
     }
   }

@@ -213,8 +213,12 @@ def test_specialised_and_generic_kernels_agree(tmp_path, train_stats):
     assert (wrapped(fast[1] - gen[1]) <= 1e-3).mean() >= 0.99
 
 
-@pytest.mark.parametrize("mode", ["argmax_enl", "reference"])
-def test_covariance_specialised_and_generic_kernels_agree(tmp_path, oracle, train_stats, mode):
+@pytest.mark.parametrize("P,S,mode", [
+    ([3, 5, 7], [1, 3], "argmax_enl"),
+    ([3, 5, 7], [1, 3], "reference"),
+    ([3, 5, 7, 9, 11], [1, 3, 5], "argmax_enl"),   # two pass shapes, staged for patch 11
+])
+def test_covariance_specialised_and_generic_kernels_agree(tmp_path, oracle, train_stats, P, S, mode):
     # 8-plane covariance input: the specialised kernel (32 x 24 tiles) against
     # the generic one, forced in a child process, up to FP32 summation order
     import os
@@ -229,18 +233,22 @@ def test_covariance_specialised_and_generic_kernels_agree(tmp_path, oracle, trai
     cov8[7] = rng.normal(0, 0.1, cov8[7].shape)
     cov8[4] *= 1.02
     cplx = (cov8[0::2] + 1j * cov8[1::2]).reshape(2, 2, 75, 90)
-    fast = dcl.nlsar(cplx, SWS, PATCHES, SCALES, train_stats, select_mode=mode)
+    st_obj = train_stats
+    if P != PATCHES or S != SCALES:
+        t1, t2, tp = synthetic.training_area(64, seed=3)
+        st_obj = dcl.nlsar_train_insar(t1, t2, tp, P, S)
+    fast = dcl.nlsar(cplx, SWS, P, S, st_obj, select_mode=mode)
     f = tmp_path / "in.pkl"
     stats = {k: (v.lut_size, v.dissims_min, v.dissims_max, v.quantilles, v.chi2cdf_inv)
-             for k, v in train_stats.items()}
+             for k, v in st_obj.items()}
     pickle.dump((cplx, stats), open(f, "wb"))
     code = (
         "import pickle,sys,numpy as np; sys.path.insert(0, %r); import despeckcl_b200 as d; "
         "c,st=pickle.load(open(%r,'rb')); "
         "st={k: d.Stats(*v) for k,v in st.items()}; "
-        "r=d.nlsar(c,21,[3,5,7],[1,3],st,select_mode=%r); "
+        "r=d.nlsar(c,21,%r,%r,st,select_mode=%r); "
         "pickle.dump(r, open(%r,'wb'))" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), str(f),
-                                          mode, str(tmp_path / "out.pkl")))
+                                          P, S, mode, str(tmp_path / "out.pkl")))
     env = dict(os.environ, DESPECKCL_B200_GENERIC="1")
     subprocess.run([sys.executable, "-c", code], env=env, check=True)
     gen = pickle.load(open(tmp_path / "out.pkl", "rb"))
@@ -536,13 +544,14 @@ def test_covariance_3x3_path_matches_oracle(oracle, mode, sws, patches):
     ((37, 29), 11, [3, 5], [1], None),          # generic kernel, one band
     ((150, 47), 11, [3, 5], [1, 3], 5),         # generic kernel, host call in 5 row bands
     ((170, 53), 21, [3, 5, 7], [1, 3], 4),      # specialised kernel, 4 bands
+    ((60, 44), 21, [3, 5, 7, 9, 11], [1, 3, 5], None),  # patches up to 11: the generic 3x3 kernel
 ])
 def test_covariance_3x3_device_entry_point_equals_host(oracle, monkeypatch, shape, sws, patches, scales, bands):
     if bands is not None:
         monkeypatch.setenv("DESPECKCL_B200_BANDS", str(bands))
     H, W = shape
-    tp, _ = _polsar_scene(32, 32, 43, homogeneous=True)
-    stats = oracle.training_covmat(tp, [3, 5, 7], [1, 3])
+    tp, _ = _polsar_scene(40, 40, 43, homogeneous=True)
+    stats = oracle.training_covmat(tp, sorted(set(patches) | {3, 5, 7}), sorted(set(scales) | {1, 3}))
     planes, cplx = _polsar_scene(H, W, 44)
     host = dcl.nlsar(cplx, sws, patches, scales, stats, select_mode="argmax_enl")
     hi = np.empty_like(planes)
