@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(kT3Threads, 1) nlsar3_kernel(const FilterParam
   }
 }
 
-// ---- specialised kernel: search window 21, patches {3,5,7} or one of them --
+// ---- specialised kernel: search window 21, patches {3,5,7} or one of them,
+// or {3,5,7} and {9,11} per scale ---------------------------------------------
 //
 // Same tile (32 x 8 outputs) and the same phases as nlsar3_kernel, with the
 // window and patch sizes fixed at compile time and two threads per output
@@ -378,8 +379,9 @@ __global__ void __launch_bounds__(kT3Threads, 1) nlsar3_kernel(const FilterParam
 // accumulators per patch size), group 1 those of the other nine planes, so a
 // thread holds at most 42 accumulators and the CTA runs 16 warps.  Group 0
 // selects; its choice reaches group 1 through shared memory once per pass.
-// Offsets run in window rows three at a time as in the 2x2 specialised
-// kernel; the measure is evaluated symmetrically in its two pixels
+// Offsets run in window rows seven (with patches up to 11: three) at a time
+// as in the 2x2 specialised kernel; the tile is staged for the call's largest
+// patch, a pass with smaller patches reading its region further in; the measure is evaluated symmetrically in its two pixels
 // ((ln det A + ln det B) first), the index of the composite weight by a
 // saturating FMA and a round-toward-zero add (the reference's `(unsigned)`
 // truncation), and the centre offset has weight 1 inside the sweep.
@@ -397,31 +399,31 @@ __host__ __device__ constexpr int group_plane(int g, int q) {
 // position of diagonal d within group 0's planes
 __host__ __device__ constexpr int diag_slot(int d) { return d == 0 ? 0 : d == 1 ? 5 : 8; }
 
-template <int PH0, int PH1, int PH2>
+// Shared-memory layout of the specialised 3x3 kernel: staging halo PHX_ (the
+// call's largest patch half), at most NPX_ patch sizes per pass.
+template <int PHX_, int NPX_>
 struct Fast3 {
-  static constexpr int WSH = 10;
-  static constexpr int NP = (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
-  static constexpr int PHM = PH2 >= 0 ? PH2 : (PH1 >= 0 ? PH1 : PH0);
+  static constexpr int WSH = 10, PHX = PHX_, NPX = NPX_;
   static constexpr int TH = kT3H, TW = kT3W;
   static constexpr int THREADS = 2 * 32 * TH;  // two groups of one warp per row
-  static constexpr int K = 7;                  // offsets per batch along a window row
+  // offsets per batch along a window row: seven with the small halo, three
+  // with the large one, which keeps L1 room for the neighbour planes
+  static constexpr int K = PHX <= 3 ? 7 : 3;
   static constexpr int NA = 14;                // accumulators per patch size (group 1 uses 9)
-  static constexpr int RS = TW + 2 * (PHM + WSH), RSH = TH + 2 * (PHM + WSH);
+  static constexpr int RS = TW + 2 * (PHX + WSH), RSH = TH + 2 * (PHX + WSH);
   static constexpr int RN = RS * RSH;
-  static constexpr int SIMW = TW + 2 * PHM, SIMH = TH + 2 * PHM;
-  static constexpr int SIMP = (SIMW + 7) / 8 * 8;
-  static constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;
-  static constexpr int HPL = K * SIMH * TW;   // one patch size's horizontal-sum plane
+  static constexpr int SIMWX = TW + 2 * PHX, SIMHX = TH + 2 * PHX;
+  static constexpr int SIMPX = (SIMWX + 7) / 8 * 8;
+  static constexpr int HPL = K * SIMHX * TW;  // one patch size's horizontal-sum plane
   static constexpr int LUTREP = 8;            // interleaved LUT copies (four lanes per copy)
   static constexpr int OFF_S9 = 0;            // [9][RSH][RS]
   static constexpr int OFF_LD = OFF_S9 + 9 * RN;
   static constexpr int OFF_SIM = OFF_LD + RN;  // [K][SIMH][SIMP]
-  static constexpr int OFF_H = OFF_SIM + K * SIMH * SIMP;
-  static constexpr int OFF_LUT = OFF_H + NP * HPL;
-  static constexpr int OFF_X = OFF_LUT + NP * kMaxLut * LUTREP;  // group 0 -> group 1: take, alpha, s0
+  static constexpr int OFF_H = OFF_SIM + K * SIMHX * SIMPX;
+  static constexpr int OFF_LUT = OFF_H + NPX * HPL;
+  static constexpr int OFF_X = OFF_LUT + NPX * kMaxLut * LUTREP;  // group 0 -> group 1: take, alpha, s0
   static constexpr int WORDS = OFF_X + 3 * 32 * TH;
   static_assert((2 * WSH + 1) % K == 0, "offset batches must tile a window row");
-  static_assert(SIMP >= 4 * 7 + 4 * NQ4, "phase-B segments must stay inside a row");
   static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
 };
 
@@ -431,37 +433,276 @@ __device__ __forceinline__ constexpr int ph3_of(int j) {
 }
 
 template <int PH0, int PH1, int PH2>
-__global__ void __launch_bounds__(Fast3<PH0, PH1, PH2>::THREADS, 1)
+__host__ __device__ constexpr int np3_of() {
+  return (PH0 >= 0) + (PH1 >= 0) + (PH2 >= 0);
+}
+
+__host__ __device__ constexpr int cmax3(int a, int b) { return a > b ? a : b; }
+
+// Selection state of one thread's pixel: group 0 keeps the weighted sums of
+// its nine planes and decides; group 1 keeps its nine planes' sums.
+struct Best3 {
+  float m[9];
+  float e, a, s0;
+  int rank, combo;
+};
+
+// One pass (one scale, patch halves PH0 < PH1 < PH2, -1 unused) of the 3x3
+// kernel over all offsets on the staged tile; a pass with smaller patches
+// than the call's largest reads its region CO pixels further in.
+template <class L, int PH0, int PH1, int PH2>
+__device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassParams& pp, float* smem, const Scene3& S,
+                                           size_t cfi, Best3& best) {
+  constexpr int WSH = L::WSH, K = L::K, NA = L::NA, RS = L::RS, RN = L::RN, TW = L::TW, NT = L::THREADS;
+  constexpr int NP = np3_of<PH0, PH1, PH2>();
+  constexpr int PHM = cmax3(PH0, cmax3(PH1, PH2));
+  constexpr int CO = L::PHX - PHM;
+  constexpr int SIMW = TW + 2 * PHM, SIMH = L::TH + 2 * PHM;
+  constexpr int SIMP = (SIMW + 7) / 8 * 8;
+  constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;
+  static_assert(PH0 >= 1 && NP <= L::NPX && CO >= 0, "pass shape");
+  static_assert(SIMP >= 4 * 7 + 4 * NQ4 && SIMP <= L::SIMPX, "phase-B segments must stay inside a row");
+  const float* sS9 = smem + L::OFF_S9;
+  const float* sLd = smem + L::OFF_LD;
+  float* sSim = smem + L::OFF_SIM;
+  float* sH = smem + L::OFF_H;
+  float* sLut = smem + L::OFF_LUT;
+  int* sTake = reinterpret_cast<int*>(smem + L::OFF_X);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = warp / L::TH, y = warp - grp * L::TH;  // warp-uniform group, output row
+  const int px = y * 32 + lane;
+  const float c2d = P.c2d;
+
+  for (int i = tid; i < NP * kMaxLut * L::LUTREP; i += NT) {
+    const int j = i / (kMaxLut * L::LUTREP);
+    const int e = (i - j * kMaxLut * L::LUTREP) / L::LUTREP;
+    sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
+  }
+  float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
+  const float* lut_j[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const ComboParams& cp = P.combo[pp.combo[j]];
+    inv_span[j] = 1.0f / cp.span;
+    nbias[j] = -cp.dmin * inv_span[j];
+    lm1[j] = cp.lm1;
+    dmax[j] = cp.dmax;
+    lut_j[j] = sLut + j * kMaxLut * L::LUTREP + (lane & (L::LUTREP - 1));
+  }
+  float acc[NP][NA];
+#pragma unroll
+  for (int j = 0; j < NP; ++j)
+#pragma unroll
+    for (int a = 0; a < NA; ++a) acc[j][a] = 0.0f;
+  __syncthreads();
+
+  for (int dy = -WSH; dy <= WSH; ++dy) {
+    for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
+      // ---- A: 3x3 similarities of offsets (dy, dx0..dx0+K-1) on the tile
+      // plus patch halo (sim_measures.h:66-160), one pixel per item
+      for (int it = tid; it < SIMH * SIMP; it += NT) {
+        const int r = it / SIMP;
+        const int c = it - r * SIMP;
+        if (c >= SIMW) continue;
+        const int ci = (r + WSH + CO) * RS + (c + WSH + CO);
+        float a[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) a[q] = sS9[q * RN + ci];
+        const float la = sLd[ci];
+        const int ni = ci + dy * RS + dx0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          float sum[9];
+#pragma unroll
+          for (int q = 0; q < 9; ++q) sum[q] = a[q] + sS9[q * RN + ni + k];
+          const float t = (la + sLd[ni + k]) + c2d;
+          float sim = fmaf(2.0f * 0.69314718f, __log2f(det3f(sum)), -t);
+          if (sim != sim) sim = 0.0f;
+          sSim[k * SIMH * SIMP + it] = sim;
+        }
+      }
+      __syncthreads();
+      // ---- B: horizontal sums of every patch size (nested rings), 4 output
+      // columns per item, a quarter warp per row
+      {
+        constexpr int QUADS = (SIMH + 3) / 4;
+        const int r_off = lane >> 3, seg = lane & 7;
+        for (int q = warp; q < K * QUADS; q += NT / 32) {
+          const int k = q / QUADS;
+          const int r = (q - k * QUADS) * 4 + r_off;
+          if (r < SIMH) {
+            const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
+            float s[4 * NQ4];
+#pragma unroll
+            for (int q4 = 0; q4 < NQ4; ++q4) {
+              const float4 v = row[q4];
+              s[4 * q4] = v.x;
+              s[4 * q4 + 1] = v.y;
+              s[4 * q4 + 2] = v.z;
+              s[4 * q4 + 3] = v.w;
+            }
+            float hs[NP][4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              float h[3] = {0.f, 0.f, 0.f};
+              float ring = s[o + PHM];
+#pragma unroll
+              for (int b = 1; b <= PHM; ++b) {
+                ring += s[o + PHM - b] + s[o + PHM + b];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                  if (ph3_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
+              }
+#pragma unroll
+              for (int j = 0; j < NP; ++j) hs[j][o] = h[j];
+            }
+#pragma unroll
+            for (int j = 0; j < NP; ++j)
+              *reinterpret_cast<float4*>(sH + j * L::HPL + (k * SIMH + r) * TW + 4 * seg) =
+                  make_float4(hs[j][0], hs[j][1], hs[j][2], hs[j][3]);
+          }
+        }
+      }
+      __syncthreads();
+      // ---- C: vertical sums, weights, this group's accumulators
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int dx = dx0 + k;
+        float w[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          const int ph = ph3_of<PH0, PH1, PH2>(j);
+          const float* col = sH + j * L::HPL + (k * SIMH + y + PHM - ph) * TW + lane;
+          float d = col[0];
+#pragma unroll
+          for (int a = 1; a <= 2 * ph3_of<PH0, PH1, PH2>(j); ++a) d += col[a * TW];
+          // compute_weights.cl:40-51 through the composite weight table
+          const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
+          const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
+          const int idx = __float_as_int(t) - 0x4B000000;
+          const float lw = lut_j[j][idx * L::LUTREP];
+          w[j] = (d > dmax[j]) ? 0.0f : lw;
+          if (dy == 0 && dx == 0) w[j] = 1.0f;
+        }
+        const size_t nfi = cfi + (ptrdiff_t)dy * S.pitch + dx;
+        float v[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+          v[q] = __ldg(S.c18 + (grp == 0 ? group_plane(0, q) : group_plane(1, q)) * S.plane + nfi);
+        if (grp == 0) {
+          float i2[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) i2[d] = v[diag_slot(d)] * v[diag_slot(d)];
+#pragma unroll
+          for (int j = 0; j < NP; ++j) {
+            acc[j][0] += w[j];
+            acc[j][1] = fmaf(w[j], w[j], acc[j][1]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[j][2 + d] = fmaf(w[j], i2[d], acc[j][2 + d]);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[j][5 + q] = fmaf(w[j], v[q], acc[j][5 + q]);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < NP; ++j)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[j][q] = fmaf(w[j], v[q], acc[j][q]);
+        }
+      }
+    }
+  }
+
+  // ---- statistics over the three diagonal intensities, alpha, ENL',
+  // selection (compute_nl_statistics.cl:92-101, compute_alphas.cl:30-41,
+  // compute_enls_nobias.cl:19-22, best_params.cpp); group 0 decides
+  if (grp == 0) {
+    int taken = -1;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      const float* A = acc[j];
+      const float s0 = A[0], s1 = A[1];
+      const float enl = s0 * s0 / s1;
+      float alpha = 0.0f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float in = A[5 + diag_slot(d)] / s0;
+        const float var = A[2 + d] / s0 - in * in;
+        alpha = fmaxf(alpha, fmaxf(0.0f, (var - in * in) / var));
+      }
+      if (P.alpha_zero) alpha = 0.0f;
+      const float oma = 1.0f - alpha;
+      const float enb = enl / (oma * oma + (alpha * alpha + 2.0f * alpha * (1.0f - alpha) / s0) * enl);
+      const int combo = pp.combo[j];
+      const int rank = P.combo[combo].rank;
+      const bool take = (P.select_mode == 0) || (enb > best.e) || (enb == best.e && rank < best.rank);
+      const bool take_fb = !take && best.combo < 0 && combo == P.fallback_combo;
+      if (take) {
+        best.e = enb;
+        best.rank = rank;
+      }
+      if (take || take_fb) {
+        best.combo = combo;
+        best.a = alpha;
+        best.s0 = s0;
+        taken = j;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) best.m[q] = A[5 + q];
+      }
+    }
+    sTake[px] = taken;
+  }
+  __syncthreads();
+  if (grp == 1) {
+    const int taken = sTake[px];
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
+      if (taken == j) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) best.m[q] = acc[j][q];
+      }
+  }
+}
+
+template <int PH0, int PH1, int PH2>
+__device__ __forceinline__ bool pass3_is(const PassParams& pp) {
+  constexpr int NP = np3_of<PH0, PH1, PH2>();
+  return pp.np == NP && pp.ph[0] == PH0 && (NP < 2 || pp.ph[1] == PH1) && (NP < 3 || pp.ph[2] == PH2);
+}
+
+template <int PHX, int A0, int A1, int A2, int B0, int B1, int B2>
+struct Fast3K {
+  using L = Fast3<PHX, cmax3(np3_of<A0, A1, A2>(), np3_of<B0, B1, B2>())>;
+};
+
+// passes of shape A and, where B0 >= 0, of shape B, staged for patch half PHX
+template <int PHX, int A0, int A1, int A2, int B0, int B1, int B2>
+__global__ void __launch_bounds__(Fast3K<PHX, A0, A1, A2, B0, B1, B2>::L::THREADS, 1)
     nlsar3_fast_kernel(const FilterParams P, const Scene3 S) {
-  using C = Fast3<PH0, PH1, PH2>;
-  constexpr int WSH = C::WSH, NP = C::NP, PHM = C::PHM, K = C::K, NA = C::NA, RS = C::RS, RN = C::RN;
-  constexpr int SIMW = C::SIMW, SIMH = C::SIMH, SIMP = C::SIMP, TW = C::TW, NT = C::THREADS;
+  using L = typename Fast3K<PHX, A0, A1, A2, B0, B1, B2>::L;
+  constexpr int WSH = L::WSH, RS = L::RS, RN = L::RN, TW = L::TW, NT = L::THREADS;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
-  float* sS9 = smem + C::OFF_S9;
-  float* sLd = smem + C::OFF_LD;
-  float* sSim = smem + C::OFF_SIM;
-  float* sH = smem + C::OFF_H;
-  float* sLut = smem + C::OFF_LUT;
-  int* sTake = reinterpret_cast<int*>(smem + C::OFF_X);
-  float* sAlpha = smem + C::OFF_X + 32 * C::TH;
-  float* sS0 = smem + C::OFF_X + 64 * C::TH;
+  float* sS9 = smem + L::OFF_S9;
+  float* sLd = smem + L::OFF_LD;
+  float* sAlpha = smem + L::OFF_X + 32 * L::TH;
+  float* sS0 = smem + L::OFF_X + 64 * L::TH;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grp = warp / C::TH, y = warp - grp * C::TH;  // warp-uniform group, output row
+  const int grp = warp / L::TH, y = warp - grp * L::TH;  // warp-uniform group, output row
   const int px = y * 32 + lane;
   const int lt = blockIdx.x + S.tile_skip;
   const int ty = lt / S.tiles_x, tx = lt - ty * S.tiles_x;
-  const int vy0 = ty * C::TH, vx0 = tx * TW;
+  const int vy0 = ty * L::TH, vx0 = tx * TW;
   const int G = P.G;
   const size_t cfi = (size_t)(vy0 + y + G) * S.pitch + (vx0 + lane + G);
-  const float c2d = P.c2d;
 
-  float acc[NP][NA];
-  float best_m[9];
-  float best_e = -1.0f, best_a = 0.0f, best_s0 = 1.0f;
-  int best_rank = 0x7fffffff, best_combo = -1;
+  Best3 best;
+  best.e = -1.0f;
+  best.a = 0.0f;
+  best.s0 = 1.0f;
+  best.rank = 0x7fffffff;
+  best.combo = -1;
 #pragma unroll
-  for (int q = 0; q < 9; ++q) best_m[q] = 0.0f;
+  for (int q = 0; q < 9; ++q) best.m[q] = 0.0f;
 
   int loaded_slot = -1;
   for (int ps = 0; ps < P.npass; ++ps) {
@@ -470,7 +711,7 @@ __global__ void __launch_bounds__(Fast3<PH0, PH1, PH2>::THREADS, 1)
     if (pp.scale_slot != loaded_slot) {
       const float* s9 = S.s9[pp.scale_slot];
       const float* ldp = S.ld[pp.scale_slot];
-      const int by = vy0 - PHM - WSH + G, bx = vx0 - PHM - WSH + G;
+      const int by = vy0 - PHX - WSH + G, bx = vx0 - PHX - WSH + G;
       for (int i = tid; i < RN; i += NT) {
         const int r = i / RS, c = i - r * RS;
         const size_t g = (size_t)(by + r) * S.pitch + (bx + c);
@@ -480,198 +721,20 @@ __global__ void __launch_bounds__(Fast3<PH0, PH1, PH2>::THREADS, 1)
       }
       loaded_slot = pp.scale_slot;
     }
-    for (int i = tid; i < NP * kMaxLut * C::LUTREP; i += NT) {
-      const int j = i / (kMaxLut * C::LUTREP);
-      const int e = (i - j * kMaxLut * C::LUTREP) / C::LUTREP;
-      sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
-    }
-    float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
-    const float* lut_j[NP];
-#pragma unroll
-    for (int j = 0; j < NP; ++j) {
-      const ComboParams& cp = P.combo[pp.combo[j]];
-      inv_span[j] = 1.0f / cp.span;
-      nbias[j] = -cp.dmin * inv_span[j];
-      lm1[j] = cp.lm1;
-      dmax[j] = cp.dmax;
-      lut_j[j] = sLut + j * kMaxLut * C::LUTREP + (lane & (C::LUTREP - 1));
-    }
-#pragma unroll
-    for (int j = 0; j < NP; ++j)
-#pragma unroll
-      for (int a = 0; a < NA; ++a) acc[j][a] = 0.0f;
-    __syncthreads();
-
-    for (int dy = -WSH; dy <= WSH; ++dy) {
-      for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
-        // ---- A: 3x3 similarities of offsets (dy, dx0..dx0+K-1) on the tile
-        // plus patch halo (sim_measures.h:66-160), one pixel per item
-        for (int it = tid; it < SIMH * SIMP; it += NT) {
-          const int r = it / SIMP;
-          const int c = it - r * SIMP;
-          if (c >= SIMW) continue;
-          const int ci = (r + WSH) * RS + (c + WSH);
-          float a[9];
-#pragma unroll
-          for (int q = 0; q < 9; ++q) a[q] = sS9[q * RN + ci];
-          const float la = sLd[ci];
-          const int ni = ci + dy * RS + dx0;
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            float sum[9];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) sum[q] = a[q] + sS9[q * RN + ni + k];
-            const float t = (la + sLd[ni + k]) + c2d;
-            float sim = fmaf(2.0f * 0.69314718f, __log2f(det3f(sum)), -t);
-            if (sim != sim) sim = 0.0f;
-            sSim[k * SIMH * SIMP + it] = sim;
-          }
-        }
-        __syncthreads();
-        // ---- B: horizontal sums of every patch size (nested rings), 4 output
-        // columns per item, a quarter warp per row
-        {
-          constexpr int QUADS = (SIMH + 3) / 4;
-          const int r_off = lane >> 3, seg = lane & 7;
-          for (int q = warp; q < K * QUADS; q += NT / 32) {
-            const int k = q / QUADS;
-            const int r = (q - k * QUADS) * 4 + r_off;
-            if (r < SIMH) {
-              const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
-              float s[4 * C::NQ4];
-#pragma unroll
-              for (int q4 = 0; q4 < C::NQ4; ++q4) {
-                const float4 v = row[q4];
-                s[4 * q4] = v.x;
-                s[4 * q4 + 1] = v.y;
-                s[4 * q4 + 2] = v.z;
-                s[4 * q4 + 3] = v.w;
-              }
-              float hs[NP][4];
-#pragma unroll
-              for (int o = 0; o < 4; ++o) {
-                float h[3] = {0.f, 0.f, 0.f};
-                float ring = s[o + PHM];
-#pragma unroll
-                for (int b = 1; b <= PHM; ++b) {
-                  ring += s[o + PHM - b] + s[o + PHM + b];
-#pragma unroll
-                  for (int j = 0; j < 3; ++j)
-                    if (ph3_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
-                }
-#pragma unroll
-                for (int j = 0; j < NP; ++j) hs[j][o] = h[j];
-              }
-#pragma unroll
-              for (int j = 0; j < NP; ++j)
-                *reinterpret_cast<float4*>(sH + j * C::HPL + (k * SIMH + r) * TW + 4 * seg) =
-                    make_float4(hs[j][0], hs[j][1], hs[j][2], hs[j][3]);
-            }
-          }
-        }
-        __syncthreads();
-        // ---- C: vertical sums, weights, this group's accumulators
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int dx = dx0 + k;
-          float w[NP];
-#pragma unroll
-          for (int j = 0; j < NP; ++j) {
-            const int ph = ph3_of<PH0, PH1, PH2>(j);
-            const float* col = sH + j * C::HPL + (k * SIMH + y + PHM - ph) * TW + lane;
-            float d = col[0];
-#pragma unroll
-            for (int a = 1; a <= 2 * ph3_of<PH0, PH1, PH2>(j); ++a) d += col[a * TW];
-            // compute_weights.cl:40-51 through the composite weight table
-            const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
-            const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
-            const int idx = __float_as_int(t) - 0x4B000000;
-            const float lw = lut_j[j][idx * C::LUTREP];
-            w[j] = (d > dmax[j]) ? 0.0f : lw;
-            if (dy == 0 && dx == 0) w[j] = 1.0f;
-          }
-          const size_t nfi = cfi + (ptrdiff_t)dy * S.pitch + dx;
-          float v[9];
-#pragma unroll
-          for (int q = 0; q < 9; ++q) v[q] = __ldg(S.c18 + (grp == 0 ? group_plane(0, q) : group_plane(1, q)) * S.plane + nfi);
-          if (grp == 0) {
-            float i2[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) i2[d] = v[diag_slot(d)] * v[diag_slot(d)];
-#pragma unroll
-            for (int j = 0; j < NP; ++j) {
-              acc[j][0] += w[j];
-              acc[j][1] = fmaf(w[j], w[j], acc[j][1]);
-#pragma unroll
-              for (int d = 0; d < 3; ++d) acc[j][2 + d] = fmaf(w[j], i2[d], acc[j][2 + d]);
-#pragma unroll
-              for (int q = 0; q < 9; ++q) acc[j][5 + q] = fmaf(w[j], v[q], acc[j][5 + q]);
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < NP; ++j)
-#pragma unroll
-              for (int q = 0; q < 9; ++q) acc[j][q] = fmaf(w[j], v[q], acc[j][q]);
-          }
-        }
-      }
-    }
-
-    // ---- statistics over the three diagonal intensities, alpha, ENL',
-    // selection (compute_nl_statistics.cl:92-101, compute_alphas.cl:30-41,
-    // compute_enls_nobias.cl:19-22, best_params.cpp); group 0 decides
-    if (grp == 0) {
-      int taken = -1;
-#pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const float* A = acc[j];
-        const float s0 = A[0], s1 = A[1];
-        const float enl = s0 * s0 / s1;
-        float alpha = 0.0f;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float in = A[5 + diag_slot(d)] / s0;
-          const float var = A[2 + d] / s0 - in * in;
-          alpha = fmaxf(alpha, fmaxf(0.0f, (var - in * in) / var));
-        }
-        if (P.alpha_zero) alpha = 0.0f;
-        const float oma = 1.0f - alpha;
-        const float enb = enl / (oma * oma + (alpha * alpha + 2.0f * alpha * (1.0f - alpha) / s0) * enl);
-        const int combo = pp.combo[j];
-        const int rank = P.combo[combo].rank;
-        const bool take = (P.select_mode == 0) || (enb > best_e) || (enb == best_e && rank < best_rank);
-        const bool take_fb = !take && best_combo < 0 && combo == P.fallback_combo;
-        if (take) {
-          best_e = enb;
-          best_rank = rank;
-        }
-        if (take || take_fb) {
-          best_combo = combo;
-          best_a = alpha;
-          best_s0 = s0;
-          taken = j;
-#pragma unroll
-          for (int q = 0; q < 9; ++q) best_m[q] = A[5 + q];
-        }
-      }
-      sTake[px] = taken;
-    }
-    __syncthreads();
-    if (grp == 1) {
-      const int taken = sTake[px];
-#pragma unroll
-      for (int j = 0; j < NP; ++j)
-        if (taken == j) {
-#pragma unroll
-          for (int q = 0; q < 9; ++q) best_m[q] = acc[j][q];
-        }
+    if constexpr (B0 < 0) {
+      fast3_pass<L, A0, A1, A2>(P, pp, smem, S, cfi, best);
+    } else {
+      if (pass3_is<A0, A1, A2>(pp))
+        fast3_pass<L, A0, A1, A2>(P, pp, smem, S, cfi, best);
+      else
+        fast3_pass<L, B0, B1, B2>(P, pp, smem, S, cfi, best);
     }
   }
 
   // ---- blend with the centre (weighted_means.cl:79), nine planes per group
   if (grp == 0) {
-    sAlpha[px] = best_a;
-    sS0[px] = best_s0;
+    sAlpha[px] = best.a;
+    sS0[px] = best.s0;
   }
   __syncthreads();
   const int vy = vy0 + y, vx = vx0 + lane;
@@ -685,46 +748,60 @@ __global__ void __launch_bounds__(Fast3<PH0, PH1, PH2>::THREADS, 1)
   for (int q = 0; q < 9; ++q) {
     const int p = grp == 0 ? group_plane(0, q) : group_plane(1, q);
     const float cp = __ldg(S.c18 + p * S.plane + cfi);
-    S.out[p * n + o] = oma * best_m[q] / s0 + alpha * cp;
+    S.out[p * n + o] = oma * best.m[q] / s0 + alpha * cp;
   }
 }
 
-template <int PH0, int PH1, int PH2>
+template <int PHX, int A0, int A1, int A2, int B0, int B1, int B2>
 cudaError_t launch3_fast_t(const FilterParams& F, const Scene3& S, unsigned tiles, cudaStream_t st) {
-  using C = Fast3<PH0, PH1, PH2>;
-  const size_t smem = (size_t)C::WORDS * 4;
+  using L = typename Fast3K<PHX, A0, A1, A2, B0, B1, B2>::L;
+  const size_t smem = (size_t)L::WORDS * 4;
   static size_t allowed[kMaxDevices];
-  const cudaError_t e = allow_dynamic_smem((const void*)nlsar3_fast_kernel<PH0, PH1, PH2>, smem, allowed);
+  const void* fn = (const void*)nlsar3_fast_kernel<PHX, A0, A1, A2, B0, B1, B2>;
+  const cudaError_t e = allow_dynamic_smem(fn, smem, allowed);
   if (e != cudaSuccess) return e;
-  nlsar3_fast_kernel<PH0, PH1, PH2><<<tiles, C::THREADS, smem, st>>>(F, S);
+  nlsar3_fast_kernel<PHX, A0, A1, A2, B0, B1, B2><<<tiles, L::THREADS, smem, st>>>(F, S);
   return cudaGetLastError();
 }
 
-// whether the specialised 3x3 kernel has the call's pass shapes: every pass
-// the patch halves {1,2,3}, or every pass one and the same half 1..3
-bool fast3_supported(const FilterParams& F) {
-  if (F.wsh != 10 || F.npass < 1) return false;
-  const PassParams& p0 = F.pass[0];
+// pass shapes of the specialised 3x3 kernel: 1 every pass {1,2,3}; 2..4 every
+// pass the single half 1..3; 5 every pass {1,2,3} or {4,5} with at least one
+// {4,5} (patches 3..11 at each scale); 0 none of these
+int fast3_shape(const FilterParams& F) {
+  if (F.wsh != 10 || F.npass < 1) return 0;
+  auto is = [](const PassParams& p, int n, int a0, int a1, int a2) {
+    return p.np == n && p.ph[0] == a0 && (n < 2 || p.ph[1] == a1) && (n < 3 || p.ph[2] == a2);
+  };
+  bool all123 = true, mix = true, any45 = false, single = true;
+  const int h0 = F.pass[0].ph[0];
   for (int i = 0; i < F.npass; ++i) {
     const PassParams& p = F.pass[i];
-    if (p.np != p0.np) return false;
-    for (int j = 0; j < p.np; ++j)
-      if (p.ph[j] != p0.ph[j]) return false;
+    const bool s123 = is(p, 3, 1, 2, 3), s45 = is(p, 2, 4, 5, -1);
+    all123 = all123 && s123;
+    mix = mix && (s123 || s45);
+    any45 = any45 || s45;
+    single = single && p.np == 1 && p.ph[0] == h0;
   }
-  if (p0.np == 3) return p0.ph[0] == 1 && p0.ph[1] == 2 && p0.ph[2] == 3;
-  return p0.np == 1 && p0.ph[0] >= 1 && p0.ph[0] <= 3;
+  if (all123) return 1;
+  if (single && h0 >= 1 && h0 <= 3) return 1 + h0;
+  if (mix && any45) return 5;
+  return 0;
 }
+
+// whether the specialised 3x3 kernel has the call's pass shapes
+bool fast3_supported(const FilterParams& F) { return fast3_shape(F) != 0; }
 
 // the specialised 3x3 kernel, for the plans fast3_supported() accepts
 cudaError_t launch3_fast(const FilterParams& F, const Scene3& S, unsigned tiles, cudaStream_t st) {
-  const PassParams& p0 = F.pass[0];
-  if (p0.np == 3) return launch3_fast_t<1, 2, 3>(F, S, tiles, st);
-  switch (p0.ph[0]) {
-    case 1: return launch3_fast_t<1, -1, -1>(F, S, tiles, st);
-    case 2: return launch3_fast_t<2, -1, -1>(F, S, tiles, st);
-    default: return launch3_fast_t<3, -1, -1>(F, S, tiles, st);
+  switch (fast3_shape(F)) {
+    case 1: return launch3_fast_t<3, 1, 2, 3, -1, -1, -1>(F, S, tiles, st);
+    case 2: return launch3_fast_t<1, 1, -1, -1, -1, -1, -1>(F, S, tiles, st);
+    case 3: return launch3_fast_t<2, 2, -1, -1, -1, -1, -1>(F, S, tiles, st);
+    case 5: return launch3_fast_t<5, 1, 2, 3, 4, 5, -1>(F, S, tiles, st);
+    default: return launch3_fast_t<3, 3, -1, -1, -1, -1, -1>(F, S, tiles, st);
   }
 }
+
 
 // ---- training ---------------------------------------------------------------
 

@@ -503,12 +503,13 @@ def test_training_3x3_matches_oracle(oracle):
 
 
 @pytest.mark.parametrize("mode", ["reference", "argmax_enl"])
-@pytest.mark.parametrize("sws,patches", [(SWS, PATCHES), (15, [3, 5])])
+@pytest.mark.parametrize("sws,patches", [(SWS, PATCHES), (15, [3, 5]), (SWS, [3, 5, 7, 9, 11])])
 def test_covariance_3x3_path_matches_oracle(oracle, mode, sws, patches):
-    # search 21 with patches {3,5,7} runs the specialised 3x3 kernel, search
-    # 15 with {3,5} the generic one
+    # search 21 with patches {3,5,7} runs the specialised 3x3 kernel, with
+    # patches 3..11 its two-pass-shape instantiation staged for patch 11,
+    # search 15 with {3,5} the generic one
     tp, _ = _polsar_scene(40, 40, 41, homogeneous=True)
-    stats = oracle.training_covmat(tp, [3, 5, 7], [1, 3])
+    stats = oracle.training_covmat(tp, sorted(set(patches) | {3, 5, 7}), [1, 3])
     planes, cplx = _polsar_scene(44, 60, 42)
     m = 0 if mode == "reference" else 1
     o = oracle.nlsar_covmat(planes, sws, patches, SCALES, stats, select_mode=m, use_double=True)
@@ -544,7 +545,7 @@ def test_covariance_3x3_path_matches_oracle(oracle, mode, sws, patches):
     ((37, 29), 11, [3, 5], [1], None),          # generic kernel, one band
     ((150, 47), 11, [3, 5], [1, 3], 5),         # generic kernel, host call in 5 row bands
     ((170, 53), 21, [3, 5, 7], [1, 3], 4),      # specialised kernel, 4 bands
-    ((60, 44), 21, [3, 5, 7, 9, 11], [1, 3, 5], None),  # patches up to 11: the generic 3x3 kernel
+    ((60, 44), 21, [3, 5, 7, 9, 11], [1, 3, 5], None),  # patches up to 11: two pass shapes
 ])
 def test_covariance_3x3_device_entry_point_equals_host(oracle, monkeypatch, shape, sws, patches, scales, bands):
     if bands is not None:
