@@ -289,6 +289,55 @@ template <typename T> struct TileOut {
   std::vector<T> bin_margin, enl_margin, var_cond, kappa, bin_margin_all;
 };
 
+// Patch sums of U pixel-similarity planes (height_sim x width_sim each) for
+// patch size p within the largest patch pmax: the row pass then the column
+// pass, each summing 2*psh+1 terms in order from 0
+// (patch_similarities_row_pass.cl:43-70, patch_similarities_col_pass.cl:43-69).
+// Output: U planes of (height_sim - pmax + 1) x (width_sim - pmax + 1).
+template <typename T>
+void patch_sums(const T* pix, int U, int Hsym, int Wo, int p, int pmax, std::vector<T>& inter, T* patch) {
+  const int psh = (p - 1) / 2, off = (pmax - p) / 2, Psh = (pmax - 1) / 2;
+  const int Hps = Hsym - pmax + 1, Wps = Wo - pmax + 1;
+  const int Hi = Hsym - 2 * off, Wi = Wps;
+  inter.assign((size_t)U * Hi * Wi, T(0));
+  for (int z = 0; z < U; ++z)
+    for (int y = 0; y < Hi; ++y)
+      for (int x = 0; x < Wi; ++x) {
+        T sum = T(0);
+        for (int k = -psh; k <= psh; ++k) sum += pix[((size_t)z * Hsym + off + y) * Wo + Psh + x + k];
+        inter[((size_t)z * Hi + y) * Wi + x] = sum;
+      }
+  for (int z = 0; z < U; ++z)
+    for (int y = 0; y < Hps; ++y)
+      for (int x = 0; x < Wps; ++x) {
+        T sum = T(0);
+        for (int k = -psh; k <= psh; ++k) sum += inter[((size_t)z * Hi + psh + y + k) * Wi + x];
+        patch[((size_t)z * Hps + y) * Wps + x] = sum;
+      }
+}
+
+// The index map of the symmetric expansion (copy_symm_weights.cl:39-77): for
+// every output pixel (hc x wc) and non-centre window offset, f(dst, src) with
+// dst the index into the full window [sws*sws][hc][wc] and src the index into
+// the upper half window [U][Hps][Wps] it copies.
+template <typename F> void symm_index_map(int hc, int wc, int sws, int Hps, int Wps, F f) {
+  const int wsh = (sws - 1) / 2, U = sws * wsh + wsh;
+  const size_t nc = (size_t)hc * wc;
+  for (int y = 0; y < hc; ++y)
+    for (int x = 0; x < wc; ++x) {
+      const size_t o = (size_t)y * wc + x;
+      for (int i = 0; i < U; ++i) f((size_t)i * nc + o, ((size_t)i * Hps + y) * Wps + x + wsh);
+      for (int hh = wsh; hh < sws; ++hh) {
+        const int ww0 = (hh == wsh) ? wsh + 1 : 0;
+        for (int ww = ww0; ww < sws; ++ww) {
+          const int hs = y + hh - wsh, ws = wsh + x + ww - wsh;
+          const int hhs = sws - hh - 1, wws = sws - ww - 1;
+          f((size_t)(hh * sws + ww) * nc + o, ((size_t)(hhs * sws + wws) * Hps + hs) * Wps + ws);
+        }
+      }
+    }
+}
+
 // nlsar_filter_sub_image.cpp:146-390 for one padded tile `ori`.
 template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterParams& P) {
   const int sws = P.sws, wsh = (sws - 1) / 2;
@@ -344,27 +393,8 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
 
     for (int p : P.patches) {
       const int ci = idx++;
-      const int psh = (p - 1) / 2, off = (pmax - p) / 2;
       const LutView& L = P.stats.at({p, s});
-      // row pass (patch_similarities_row_pass.cl:43-70)
-      const int Hi = Hsym - 2 * off, Wi = Wps;
-      inter.assign((size_t)U * Hi * Wi, T(0));
-      for (int z = 0; z < U; ++z)
-        for (int y = 0; y < Hi; ++y)
-          for (int x = 0; x < Wi; ++x) {
-            T sum = T(0);
-            for (int k = -psh; k <= psh; ++k)
-              sum += pix[((size_t)z * Hsym + off + y) * Wo + Psh + x + k];
-            inter[((size_t)z * Hi + y) * Wi + x] = sum;
-          }
-      // column pass (patch_similarities_col_pass.cl:43-69)
-      for (int z = 0; z < U; ++z)
-        for (int y = 0; y < Hps; ++y)
-          for (int x = 0; x < Wps; ++x) {
-            T sum = T(0);
-            for (int k = -psh; k <= psh; ++k) sum += inter[((size_t)z * Hi + psh + y + k) * Wi + x];
-            patch[((size_t)z * Hps + y) * Wps + x] = sum;
-          }
+      patch_sums<T>(pix.data(), U, Hsym, Wo, p, pmax, inter, patch.data());
       // weights (compute_weights.cl)
       if (P.want_diag) wmargin.assign(wsym.size(), std::numeric_limits<T>::infinity());
       for (size_t i = 0; i < wsym.size(); ++i)
@@ -372,26 +402,11 @@ template <typename T> TileOut<T> filter_tile(const Cov<T>& ori, const FilterPara
       // symmetric expansion (copy_symm_weights.cl:39-77) + self weight (routines.cpp:151-157)
       std::vector<T> fmargin;
       if (P.want_diag) fmargin.assign((size_t)N * nc, std::numeric_limits<T>::infinity());
-      for (int y = 0; y < hc; ++y)
-        for (int x = 0; x < wc; ++x) {
-          const size_t o = (size_t)y * wc + x;
-          for (int i = 0; i < U; ++i) {
-            const size_t si = ((size_t)i * Hps + y) * Wps + x + wsh;
-            wfull[(size_t)i * nc + o] = wsym[si];
-            if (P.want_diag) fmargin[(size_t)i * nc + o] = wmargin[si];
-          }
-          wfull[(size_t)U * nc + o] = T(1);
-          for (int hh = wsh; hh < sws; ++hh) {
-            const int ww0 = (hh == wsh) ? wsh + 1 : 0;
-            for (int ww = ww0; ww < sws; ++ww) {
-              const int hs = y + hh - wsh, ws = wsh + x + ww - wsh;
-              const int hhs = sws - hh - 1, wws = sws - ww - 1;
-              const size_t si = ((size_t)(hhs * sws + wws) * Hps + hs) * Wps + ws;
-              wfull[(size_t)(hh * sws + ww) * nc + o] = wsym[si];
-              if (P.want_diag) fmargin[(size_t)(hh * sws + ww) * nc + o] = wmargin[si];
-            }
-          }
-        }
+      symm_index_map(hc, wc, sws, Hps, Wps, [&](size_t dst, size_t src) {
+        wfull[dst] = wsym[src];
+        if (P.want_diag) fmargin[dst] = wmargin[src];
+      });
+      for (size_t o = 0; o < nc; ++o) wfull[(size_t)U * nc + o] = T(1);
       // statistics (compute_nl_statistics.cl:72-103), alphas, ENL'
       ComboResult<T>& R = res[ci];
       R.enl_nobias.assign(nc, 0);
@@ -815,4 +830,28 @@ extern "C" int oracle_tile_list(int H, int W, int th, int tw, int ov, int* h0, i
     w0[i] = t[i].w0;
   }
   return n;
+}
+
+// Stage entry points for the known-answer tests of the reference's kernel
+// tests (compute_patch_similarities_test.cpp:31-81,
+// copy_symm_weights_test.cpp:33-128), FP32.
+extern "C" int oracle_patch_similarities(const float* pix, float* out, int height_sim, int width_sim, int sws,
+                                         int patch_size, int patch_size_max) {
+  if (sws < 1 || sws % 2 == 0 || patch_size < 1 || patch_size % 2 == 0 || patch_size > patch_size_max ||
+      height_sim < patch_size_max || width_sim < patch_size_max)
+    return -1;
+  const int wsh = (sws - 1) / 2, U = sws * wsh + wsh;
+  std::vector<float> inter;
+  patch_sums<float>(pix, U, height_sim, width_sim, patch_size, patch_size_max, inter, out);
+  return 0;
+}
+
+extern "C" int oracle_copy_symm_weights(const float* wsymm, float* wfull, int height_ori, int width_ori, int sws) {
+  if (sws < 1 || sws % 2 == 0 || height_ori < 1 || width_ori < 1) return -1;
+  const int wsh = (sws - 1) / 2, U = sws * wsh + wsh;
+  const size_t nc = (size_t)height_ori * width_ori;
+  symm_index_map(height_ori, width_ori, sws, height_ori + wsh, width_ori + 2 * wsh,
+                 [&](size_t dst, size_t src) { wfull[dst] = wsymm[src]; });
+  for (size_t o = 0; o < nc; ++o) wfull[(size_t)U * nc + o] = 1.0f;
+  return 0;
 }

@@ -357,3 +357,101 @@ def ref_nlinsar(a1, a2, phi, sws=21, patch_size=7, niter=5, lmin=10, init=None):
     if rc:
         raise ValueError("unsupported NL-InSAR parameters")
     return ref, ph, coh
+
+
+def _ref_stats_arrays(stats):
+    """Flattened statistics for the reference shim: keys (patch, scale) in map
+    order, LUT sizes, ranges and the concatenated LUTs."""
+    items = sorted(stats.items(), key=lambda kv: (kv[0][0], kv[0][1]))
+    keys = np.int32([[k[0], k[1]] for k, _ in items]).reshape(-1)
+    sizes = np.int32([int(st.lut_size) for _, st in items])
+    dmin = np.float32([st.dissims_min for _, st in items])
+    dmax = np.float32([st.dissims_max for _, st in items])
+    quant = np.concatenate([_f32(st.quantilles)[: int(st.lut_size)] for _, st in items])
+    chi2 = np.concatenate([_f32(st.chi2cdf_inv)[: int(st.lut_size)] for _, st in items])
+    return keys, sizes, dmin, dmax, _f32(quant), _f32(chi2)
+
+
+def ref_nlsar_insar(a1, a2, phi, sws, patches, scales, stats, h=15.0, c=49.0, select_mode=0, tile=None):
+    """The reference's own NL-SAR kernels run on the CPU (oracle/_ref,
+    nlsar_ref_shim.cpp): (ref, phase, coh, sel), or None when they were not
+    built here.  select_mode 0 is the reference's get_best_params, 1 the ENL
+    argmax."""
+    R = ref_pieces()
+    if R is None:
+        return None
+    a1, a2, phi = _f32(a1), _f32(a2), _f32(phi)
+    H, W = a1.shape
+    out = [np.zeros((H, W), np.float32) for _ in range(3)]
+    sel = np.zeros((H, W), np.int32)
+    p = np.array(patches, np.int32)
+    s = np.array(scales, np.int32)
+    keys, sizes, dmin, dmax, quant, chi2 = _ref_stats_arrays(stats)
+    th, tw = tile if tile else default_tile(H, W, sws, patches, scales)
+    rc = R.ref_nlsar_insar(_fp(a1), _fp(a2), _fp(phi), _fp(out[0]), _fp(out[1]), _fp(out[2]), H, W, int(sws),
+                           _ip(p), len(p), _ip(s), len(s), _ip(keys), len(sizes), _ip(sizes), _fp(dmin), _fp(dmax),
+                           _fp(quant), _fp(chi2), ctypes.c_float(h), ctypes.c_float(c), int(select_mode), th, tw,
+                           _ip(sel))
+    if rc:
+        raise ValueError(f"ref_nlsar_insar failed: {rc}")
+    return out[0], out[1], out[2], sel
+
+
+def ref_nlsar_covmat(cov8, sws, patches, scales, stats, h=15.0, c=49.0, select_mode=0, tile=None):
+    """The reference's own NL-SAR kernels on an 8-plane 2x2 covariance image
+    ([8][H][W]), or None when they were not built here."""
+    R = ref_pieces()
+    if R is None:
+        return None
+    cov8 = _f32(cov8)
+    _, H, W = cov8.shape
+    out = np.zeros_like(cov8)
+    p = np.array(patches, np.int32)
+    s = np.array(scales, np.int32)
+    keys, sizes, dmin, dmax, quant, chi2 = _ref_stats_arrays(stats)
+    th, tw = tile if tile else default_tile(H, W, sws, patches, scales)
+    rc = R.ref_nlsar_covmat(_fp(cov8), _fp(out), H, W, int(sws), _ip(p), len(p), _ip(s), len(s), _ip(keys),
+                            len(sizes), _ip(sizes), _fp(dmin), _fp(dmax), _fp(quant), _fp(chi2), ctypes.c_float(h),
+                            ctypes.c_float(c), int(select_mode), th, tw)
+    if rc:
+        raise ValueError(f"ref_nlsar_covmat failed: {rc}")
+    return out
+
+
+def patch_similarities(pix, sws, patch_size, patch_size_max, reference=False):
+    """Patch sums of U = sws*wsh + wsh pixel-similarity planes pix
+    [U][height_sim][width_sim] (the oracle's stage, or with reference=True the
+    reference's row and column pass kernels; None when those were not built)."""
+    pix = _f32(pix)
+    U, hs, ws = pix.shape
+    out = np.zeros((U, hs - patch_size_max + 1, ws - patch_size_max + 1), np.float32)
+    if reference:
+        R = ref_pieces()
+        if R is None:
+            return None
+        rc = R.ref_patch_similarities(_fp(pix), _fp(out), hs, ws, int(sws), int(patch_size), int(patch_size_max))
+    else:
+        rc = lib().oracle_patch_similarities(_fp(pix), _fp(out), hs, ws, int(sws), int(patch_size),
+                                             int(patch_size_max))
+    if rc:
+        raise ValueError("bad patch-similarity arguments")
+    return out
+
+
+def copy_symm_weights(wsymm, height_ori, width_ori, sws, reference=False):
+    """The upper half window of weights [U][height_ori + wsh][width_ori + 2 wsh]
+    expanded to the full window [sws*sws][height_ori][width_ori] (the oracle's
+    index map, or the reference's kernel with reference=True; None when that
+    was not built)."""
+    wsymm = _f32(wsymm)
+    out = np.zeros((sws * sws, height_ori, width_ori), np.float32)
+    if reference:
+        R = ref_pieces()
+        if R is None:
+            return None
+        rc = R.ref_copy_symm_weights(_fp(wsymm), _fp(out), int(height_ori), int(width_ori), int(sws))
+    else:
+        rc = lib().oracle_copy_symm_weights(_fp(wsymm), _fp(out), int(height_ori), int(width_ori), int(sws))
+    if rc:
+        raise ValueError("bad symmetric-copy arguments")
+    return out

@@ -1,14 +1,21 @@
-"""Writes tests/golden/reference_pieces.npz: outputs of the reference's own
-code, compiled from the reference sources by oracle/Makefile into
-oracle/_ref/libref_pieces.so (the translation units that build without
-OpenCL, GSL or Boost, and the Goldstein / NL-InSAR kernels compiled as C++).
+"""Writes the golden fixtures: outputs of the reference's own code, compiled
+from the reference sources by oracle/Makefile into oracle/_ref/libref_pieces.so
+(the translation units that build without OpenCL, GSL or Boost, and the
+NL-SAR, Goldstein and NL-InSAR kernels compiled as C++).
 
     make -C oracle && python tests/golden/make_golden.py
 
-The fixtures let tests/test_golden.py pin the oracle without the reference
-tree: pixel similarities (2x2 and 3x3, sim_measures.h), the tile iterator
-(tile_iterator.cpp), the selection of best_params.cpp, and the Goldstein and
-NL-InSAR outputs of the reference's kernels on two small seeded scenes.
+tests/golden/reference_pieces.npz: pixel similarities (2x2 and 3x3,
+sim_measures.h), the tile iterator (tile_iterator.cpp), the selection of
+best_params.cpp, and the Goldstein and NL-InSAR outputs of the reference's
+kernels on two small seeded scenes.
+
+tests/golden/reference_nlsar.npz: end-to-end NL-SAR outputs of the
+reference's kernels (oracle/nlsar_ref_shim.cpp) on seeded scenes, both
+selection modes, with the statistics (LUTs) they used.
+
+The fixtures let tests/test_golden.py pin the oracle, and
+tests/test_gpu_reference_nlsar.py the CUDA path, without the reference tree.
 """
 import ctypes
 import os
@@ -88,5 +95,71 @@ def main():
     print("wrote", os.path.join(HERE, "reference_pieces.npz"))
 
 
+# NL-SAR cases: (name, H, W, seed, patches, scales, select modes, tile or None)
+NLSAR_CASES = [
+    ("s64x80", 64, 80, 41, [3, 5, 7], [1, 3], (0, 1), None),
+    ("s96x96", 96, 96, 42, [3, 5, 7], [1, 3], (0, 1), None),
+    ("example", 40, 48, 43, [3, 5, 7, 9, 11], [1, 3, 5], (0, 1), None),
+    ("tiled", 70, 90, 45, [3, 5, 7], [1, 3], (0, 1), (60, 60)),
+]
+
+
+def covariance_input(seed):
+    """A generic 2x2 covariance image [8][H][W]: the covariance of an InSAR
+    scene, 3x3 box-averaged, with an independent imaginary diagonal and a
+    perturbed lower off-diagonal, so every plane carries its own data."""
+    a1, a2, ph = synthetic.insar_scene(40, 48, seed)
+    z1 = a1.astype(np.float64)
+    z2 = a2.astype(np.float64) * np.exp(-1j * ph.astype(np.float64))
+    pad = lambda x: np.pad(x, 1, mode="edge")  # noqa: E731
+    box = lambda x: sum(pad(x)[i:i + 40, j:j + 48] for i in range(3) for j in range(3)) / 9  # noqa: E731
+    c00, c11, c01 = box(np.abs(z1) ** 2), box(np.abs(z2) ** 2), box(z1 * np.conj(z2))
+    rng = np.random.default_rng(seed)
+    cov = np.stack([c00, rng.normal(0, 0.05, c00.shape), c01.real, c01.imag, 1.01 * c01.real, -c01.imag, c11,
+                    rng.normal(0, 0.05, c00.shape)])
+    return cov.astype(np.float32)
+
+
+def nlsar_main():
+    if pyoracle.ref_pieces() is None:
+        raise SystemExit("oracle/_ref/libref_pieces.so not built: run `make -C oracle` with the reference tree present")
+    t1, t2, tp = synthetic.training_area(128, seed=7)
+    stats = pyoracle.training_insar(t1, t2, tp, [3, 5, 7, 9, 11], [1, 3, 5])
+    keys = sorted(stats)
+    out = {"stat_keys": np.int32(keys), "stat_lut_size": np.int32([stats[k].lut_size for k in keys]),
+           "stat_dmin": np.float32([stats[k].dissims_min for k in keys]),
+           "stat_dmax": np.float32([stats[k].dissims_max for k in keys]),
+           "stat_quant": np.stack([np.float32(stats[k].quantilles) for k in keys]),
+           "stat_chi2": np.stack([np.float32(stats[k].chi2cdf_inv) for k in keys])}
+    names = []
+    for name, H, W, seed, patches, scales, modes, tile in NLSAR_CASES:
+        a1, a2, ph = synthetic.insar_scene(H, W, seed)
+        st = {k: v for k, v in stats.items() if k[0] in patches and k[1] in scales}
+        out[f"{name}_in"] = np.stack([a1, a2, ph])
+        out[f"{name}_patches"] = np.int32(patches)
+        out[f"{name}_scales"] = np.int32(scales)
+        out[f"{name}_tile"] = np.int32(tile if tile else pyoracle.default_tile(H, W, 21, patches, scales))
+        for m in modes:
+            r = pyoracle.ref_nlsar_insar(a1, a2, ph, 21, patches, scales, st, select_mode=m, tile=tile)
+            out[f"{name}_m{m}_out"] = np.stack(r[:3])
+            out[f"{name}_m{m}_sel"] = r[3]
+            print(name, "mode", m, "done")
+        names.append(name)
+    out["cases"] = np.array(names)
+    cov = covariance_input(44)
+    st = {k: v for k, v in stats.items() if k[0] in (3, 5, 7) and k[1] in (1, 3)}
+    out["cov_in"] = cov
+    for m in (0, 1):
+        out[f"cov_m{m}_out"] = pyoracle.ref_nlsar_covmat(cov, 21, [3, 5, 7], [1, 3], st, select_mode=m)
+    np.savez_compressed(os.path.join(HERE, "reference_nlsar.npz"), **out)
+    print("wrote", os.path.join(HERE, "reference_nlsar.npz"))
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "nlsar":
+        nlsar_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "pieces":
+        main()
+    else:
+        main()
+        nlsar_main()

@@ -8,6 +8,7 @@ import os
 
 import numpy as np
 import pytest
+from nlsar_parity import REF_NLSAR, nlsar_cases, nlsar_stats
 
 G = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_pieces.npz"))
 
@@ -58,3 +59,39 @@ def test_nlinsar_fp32_restatement_matches_reference_bit_for_bit(oracle):
     mine = oracle.nlinsar(a1, a2, ph, 21, 7, 2, 10, use_double=False)
     for m, r in zip(mine, G["nl_ref"]):
         assert np.array_equal(m, r)
+
+
+# ---- end-to-end NL-SAR: the reference's own kernels (oracle/nlsar_ref_shim.cpp)
+
+N = REF_NLSAR
+
+
+@pytest.mark.parametrize("name,mode", list(nlsar_cases()))
+def test_nlsar_fp32_oracle_matches_reference_kernels_bit_for_bit(oracle, name, mode):
+    a1, a2, ph = N[f"{name}_in"]
+    patches, scales = list(N[f"{name}_patches"]), list(N[f"{name}_scales"])
+    st = nlsar_stats(oracle, patches, scales)
+    o = oracle.nlsar_insar(a1, a2, ph, 21, patches, scales, st, select_mode=mode, use_double=False,
+                           tile=tuple(int(t) for t in N[f"{name}_tile"]), diag=True)
+    ref = N[f"{name}_m{mode}_out"]
+    for i in range(3):
+        assert np.array_equal(o[i], ref[i], equal_nan=True), (name, mode, i, np.argwhere(o[i] != ref[i])[:5])
+    assert np.array_equal(o[3].sel, N[f"{name}_m{mode}_sel"])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_nlsar_covariance_fp32_oracle_matches_reference_kernels_bit_for_bit(oracle, mode):
+    st = nlsar_stats(oracle, [3, 5, 7], [1, 3])
+    o = oracle.nlsar_covmat(N["cov_in"], 21, [3, 5, 7], [1, 3], st, select_mode=mode, use_double=False)
+    assert np.array_equal(o, N[f"cov_m{mode}_out"], equal_nan=True)
+
+
+def test_nlsar_reference_fixtures_cover_both_modes_and_the_boundary():
+    # both selection modes differ somewhere, and the tiled case's tiles meet
+    # inside the scene (70 x 90 with 60 x 60 tiles and overlap 14)
+    a = N["s96x96_m0_out"]
+    b = N["s96x96_m1_out"]
+    assert not np.array_equal(a, b)
+    assert len(np.unique(N["s96x96_m1_sel"])) > 1
+    assert (N["s96x96_m0_sel"] == N["s96x96_m0_sel"].flat[0]).all()  # the last key everywhere
+    assert tuple(N["tiled_tile"]) == (60, 60)

@@ -22,9 +22,9 @@ pytestmark = pytest.mark.gpu
 
 import despeckcl_b200 as dcl  # noqa: E402
 from despeckcl_b200 import synthetic  # noqa: E402
+from nlsar_parity import KAPPA_MAX, PHASE_TOL, REL_TOL, check_parity, run_gpu, wrapped  # noqa: E402,F401
 
 SWS, PATCHES, SCALES = 21, [3, 5, 7], [1, 3]
-REL_TOL, PHASE_TOL = 1e-4, 1e-3
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -32,47 +32,6 @@ def _cuda():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     torch.cuda.init()
-
-
-def run_gpu(a1, a2, ph, stats, mode, sws=SWS, patches=PATCHES, scales=SCALES, selection=False):
-    t = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (a1, a2, ph)]
-    sel = torch.zeros(a1.shape, dtype=torch.int32, device="cuda") if selection else None
-    out = dcl.nlsar_insar_device(*t, sws, patches, scales, stats, select_mode=mode, selection=sel)
-    torch.cuda.synchronize()
-    res = [o.cpu().numpy() for o in out]
-    if selection:
-        res.append(sel.cpu().numpy())
-    return res
-
-
-def wrapped(d):
-    return np.abs(np.angle(np.exp(1j * d.astype(np.float64))))
-
-
-KAPPA_MAX = 20.0
-
-
-def check_parity(gpu, ora, diag, mode, min_all=0.99, min_stable=0.5):
-    ref_g, ph_g, coh_g = gpu[:3]
-    ref_o, ph_o, coh_o = ora
-    stable = (diag.bin_margin > 1e-3) & (diag.var_cond > 1e-4)
-    if mode == "argmax_enl":
-        stable &= diag.enl_margin > 1e-4
-    stable_c = stable & (diag.kappa <= KAPPA_MAX)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        e_ref = np.abs(ref_g - ref_o) / np.abs(ref_o)
-        e_coh = np.abs(coh_g - coh_o) / np.maximum(np.abs(coh_o), 1e-3)
-    e_ph = wrapped(ph_g - ph_o)
-    ok_ref = e_ref <= REL_TOL
-    ok_c = (e_coh <= REL_TOL) & (e_ph <= PHASE_TOL)
-    bad = (stable & ~ok_ref) | (stable_c & ~ok_c)
-    assert not bad.any(), (
-        f"{bad.sum()} well-conditioned pixels outside tolerance; worst rel ref {e_ref[stable].max():.3g}, "
-        f"coh {e_coh[stable_c].max():.3g}, phase {e_ph[stable_c].max():.3g}; first at {np.argwhere(bad)[:5].tolist()}")
-    ok = ok_ref & ok_c
-    assert ok.mean() >= min_all, f"only {ok.mean():.4f} of all pixels within tolerance"
-    assert stable.mean() >= min_stable
-    return ok.mean(), stable.mean()
 
 
 @pytest.mark.parametrize("mode", ["reference", "argmax_enl"])

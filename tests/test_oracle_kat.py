@@ -297,3 +297,55 @@ def test_training_3x3_pair_counts(oracle):
         d = oracle.training_dissims(cov, p, s)
         assert d.size == n * (n - 1) // 2
         assert np.isfinite(d).all()
+
+
+@pytest.mark.parametrize("reference", [False, True])
+@pytest.mark.parametrize("patch,pmax", [(3, 3), (3, 7), (5, 7)])
+def test_patch_sums_of_constant_planes(oracle, reference, patch, pmax):
+    # compute_patch_similarities_test.cpp:31-81: plane d of the pixel
+    # similarities holds d everywhere; every patch sum of plane d is d * p^2
+    # (20 x 30 similarities, search window 5).  reference=True runs the
+    # reference's row and column pass kernels (oracle/_ref), when built.
+    hs, ws, sws = 20, 30, 5
+    U = sws * (sws // 2) + sws // 2
+    pix = np.broadcast_to(np.arange(U, dtype=np.float32)[:, None, None], (U, hs, ws))
+    got = oracle.patch_similarities(pix, sws, patch, pmax, reference=reference)
+    if got is None:
+        pytest.skip("reference pieces not built")
+    want = np.broadcast_to((np.arange(U, dtype=np.float32) * patch * patch)[:, None, None], got.shape)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-4)
+
+
+def test_patch_sums_oracle_equals_reference_kernels_on_random_planes(oracle):
+    rng = np.random.default_rng(11)
+    pix = rng.gamma(2.0, 1.0, (12, 23, 29)).astype(np.float32)
+    for patch, pmax in [(3, 7), (5, 7), (7, 7), (9, 11)]:
+        ref = oracle.patch_similarities(pix, 5, patch, pmax, reference=True)
+        if ref is None:
+            pytest.skip("reference pieces not built")
+        np.testing.assert_array_equal(oracle.patch_similarities(pix, 5, patch, pmax), ref)
+
+
+@pytest.mark.parametrize("reference", [False, True])
+def test_copy_symm_weights_index_map(oracle, reference):
+    # copy_symm_weights_test.cpp:33-128: random weights 0..9 on the upper half
+    # window (70 x 30 pixels, search window 7); the full window holds the copied
+    # upper half and, for the lower half, the value of the mirrored offset at
+    # the shifted pixel.  reference=True runs the reference's kernel.
+    ho, wo, sws = 70, 30, 7
+    wsh = sws // 2
+    U = sws * wsh + wsh
+    rng = np.random.default_rng(5)
+    wsymm = rng.integers(0, 10, (U, ho + wsh, wo + 2 * wsh)).astype(np.float32)
+    full = oracle.copy_symm_weights(wsymm, ho, wo, sws, reference=reference)
+    if full is None:
+        pytest.skip("reference pieces not built")
+    for i in range(U):
+        np.testing.assert_array_equal(full[i], wsymm[i, :ho, wsh:wsh + wo])
+    for hh in range(wsh, sws):
+        for ww in range(wsh + 1 if hh == wsh else 0, sws):
+            hhs, wws = sws - hh - 1, sws - ww - 1
+            src = wsymm[hhs * sws + wws, hh - wsh:hh - wsh + ho, ww:ww + wo]
+            np.testing.assert_array_equal(full[hh * sws + ww], src)
+    if not reference:
+        np.testing.assert_array_equal(full[U], np.ones((ho, wo), np.float32))  # self weight
