@@ -78,6 +78,9 @@ def parse():
     p.add_argument("--cov-size", type=int, default=2048, help="secondary: side of the 2x2 covariance scene")
     p.add_argument("--requests", type=int, default=96, help="serving: requests per stream")
     p.add_argument("--hbm-budget-gb", type=float, default=120.0, help="serving: admission budget")
+    p.add_argument("--no-extras", action="store_true",
+                   help="plain: skip the shortened batched and served measurements beside the headline")
+    p.add_argument("--extra-requests", type=int, default=24, help="plain: requests of the served stream")
     return p.parse_args()
 
 
@@ -330,6 +333,15 @@ def run_ours(args):
     headline = PATCHES == [3, 5, 7] and SCALES == [1, 3] and args.mode == "argmax_enl"
     traffic = traffic_from_profiles(S) if headline else None
 
+    # the batched and served workloads, shortened, beside the headline (one
+    # GPU only; the headline numbers above are already taken)
+    batched = served = None
+    if args.gpus == 1 and not args.no_extras and PATCHES == [3, 5, 7] and SCALES == [1, 3]:
+        del dev, out
+        torch.cuda.empty_cache()
+        batched = batched_measure(args, stats, 3)
+        served = serving_measure(args, stats, args.extra_requests, (1.1,))
+
     cpu = None
     if rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -361,6 +373,10 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if batched:
+            line["batched"] = batched
+        if served:
+            line["serving"] = {k: v for k, v in served.items() if k != "rates"}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -375,17 +391,16 @@ def batched_scenes(n=48, lo=256, hi=2048, seed0=100):
     return [(int(rng.integers(lo, hi + 1)), int(rng.integers(lo, hi + 1)), seed0 + i) for i in range(n)]
 
 
-def run_batched(args):
+def batched_measure(args, stats, k):
     """48 interferograms of uneven size: one persistent launch per run (eager
     and as a CUDA graph, kernel instantiation picked by the autotuner) against
-    looping the plain one-scene-per-launch path over the same scenes."""
+    looping the plain one-scene-per-launch path over the same scenes; device
+    times with CUDA events on the launching stream."""
     import torch
 
     import despeckcl_b200 as dcl
     from despeckcl_b200 import synthetic
 
-    torch.cuda.set_device(0)
-    stats = make_stats(dcl, synthetic)
     spec = batched_scenes()
     scenes = []
     for h, w, seed in spec:
@@ -411,29 +426,48 @@ def run_batched(args):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / k
 
-    k = max(1, args.steps)
     ms_loop = timed(loop, k)
     eager = dcl.NlsarBatch(scenes, SWS, PATCHES, SCALES, stats, H_PARAM, C_PARAM, select_mode=args.mode, outs=outs,
                            graph=False, autotune=True)
     ms_eager = timed(lambda: eager.run(stream), k)
     graph = dcl.NlsarBatch(scenes, SWS, PATCHES, SCALES, stats, H_PARAM, C_PARAM, select_mode=args.mode, outs=outs,
                            graph=True, autotune=True)
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        ms_graph = timed(lambda: graph.run(stream), k)
-    line = {
-        "metric": "NL-SAR Mpix/s (batched)", "value": mpix / (ms_graph * 1e-3), "unit": UNIT, "n_gpus": 1,
-        "steps": k, "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{len(spec)} scenes, H and W uniform in [256, 2048], {mpix:.1f} Mpix per step",
-                   "search_window": SWS, "patches": PATCHES, "scales": SCALES, "select_mode": args.mode},
-        "plain_loop": {"value": mpix / (ms_loop * 1e-3), "ms_per_step": ms_loop},
-        "batched_eager": {"value": mpix / (ms_eager * 1e-3), "ms_per_step": ms_eager},
-        "speedup_vs_plain_loop": ms_loop / ms_graph, "kernel_variant": graph.variant,
-        "gpu_launches": graph.launches, "clocks": clk.summary(),
-    }
-    print(json.dumps(line), flush=True)
+    ms_graph = timed(lambda: graph.run(stream), k)
+    res = {"workload": f"{len(spec)} scenes, H and W uniform in [256, 2048], {mpix:.1f} Mpix per step",
+           "mpix_s": mpix / (ms_graph * 1e-3), "ms_per_step": ms_graph, "steps": k,
+           "plain_loop": {"mpix_s": mpix / (ms_loop * 1e-3), "ms_per_step": ms_loop},
+           "batched_eager": {"mpix_s": mpix / (ms_eager * 1e-3), "ms_per_step": ms_eager},
+           "speedup_vs_plain_loop": ms_loop / ms_graph, "kernel_variant": graph.variant,
+           "gpu_launches": graph.launches}
     eager.close()
     graph.close()
+    del scenes, outs
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_batched(args):
+    import torch
+
+    import despeckcl_b200 as dcl
+    from despeckcl_b200 import synthetic
+
+    torch.cuda.set_device(0)
+    stats = make_stats(dcl, synthetic)
+    k = max(1, args.steps)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        r = batched_measure(args, stats, k)
+    line = {
+        "metric": "NL-SAR Mpix/s (batched)", "value": r["mpix_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": k, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": r["workload"], "search_window": SWS, "patches": PATCHES, "scales": SCALES,
+                   "select_mode": args.mode},
+        "plain_loop": r["plain_loop"], "batched_eager": r["batched_eager"],
+        "speedup_vs_plain_loop": r["speedup_vs_plain_loop"], "kernel_variant": r["kernel_variant"],
+        "gpu_launches": r["gpu_launches"], "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -443,14 +477,13 @@ def _pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
 
-def run_serving(args):
-    """Poisson request streams (0.5, 0.8 and 1.1 times the plain path's
-    request rate) of scenes with sides uniform in [256, 4096], each request
-    seeded by its id, served by the request server (HBM-budget admission,
-    continuous batching) and, under the same arrivals, by the plain path
-    (one scene per call, one call at a time).  Inputs and outputs stay on the
-    device; latency runs from a request's arrival to the end of its last
-    launch."""
+def serving_measure(args, stats, n, factors):
+    """Poisson request streams (`factors` times the plain path's request rate)
+    of scenes with sides uniform in [256, 4096], each request seeded by its id,
+    served by the request server (HBM-budget admission, continuous batching)
+    and, under the same arrivals, by the plain path (one scene per call, one
+    call at a time).  Inputs and outputs stay on the device; latency runs from
+    a request's arrival to the end of its last launch."""
     import threading
     import time
 
@@ -460,9 +493,6 @@ def run_serving(args):
     import despeckcl_b200 as dcl
     from despeckcl_b200 import synthetic
 
-    torch.cuda.set_device(0)
-    stats = make_stats(dcl, synthetic)
-    n = args.requests
     rng = np.random.default_rng(5)
     sizes = [(int(rng.integers(256, 4097)), int(rng.integers(256, 4097))) for _ in range(n)]
     scenes = [synthetic.insar_scene_device(h, w, i) for i, (h, w) in enumerate(sizes)]
@@ -539,36 +569,54 @@ def run_serving(args):
         return {"mpix_s": px.sum() / 1e6 / span, "p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99)}
 
     rates = []
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        for k, f in enumerate((0.5, 0.8, 1.1)):
-            lam = f * mu
-            arr = np.cumsum(np.random.default_rng(1000 + k).exponential(1.0 / lam, n))
-            arr -= arr[0]
-            b0 = srv.stats()["batches"]
-            served = served_stream(arr)
-            served["batches"] = srv.stats()["batches"] - b0
-            plain = plain_stream(arr)
-            rates.append({"rate_factor": f, "offered_req_s": lam, "offered_mpix_s": lam * px.mean() / 1e6,
-                          "served": served, "plain": plain})
+    for k, f in enumerate(factors):
+        lam = f * mu
+        arr = np.cumsum(np.random.default_rng(1000 + k).exponential(1.0 / lam, n))
+        arr -= arr[0]
+        b0 = srv.stats()["batches"]
+        served = served_stream(arr)
+        served["batches"] = srv.stats()["batches"] - b0
+        plain = plain_stream(arr)
+        rates.append({"rate_factor": f, "offered_req_s": lam, "offered_mpix_s": lam * px.mean() / 1e6,
+                      "served": served, "plain": plain})
     st = srv.stats()
     srv.close()
     top = rates[-1]["served"]
+    res = {"workload": f"{n} requests per stream, sides uniform in [256, 4096], {px.sum() / 1e6:.0f} Mpix per stream",
+           "hbm_budget_gb": args.hbm_budget_gb, "max_inflight": 2, "max_batch_tiles": 148 * 8,
+           "rate_factor": factors[-1], "mpix_s": top["mpix_s"], "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+           "plain_p50_ms": rates[-1]["plain"]["p50_ms"], "plain_p99_ms": rates[-1]["plain"]["p99_ms"],
+           "capacity": {"plain_mpix_s": px.sum() / 1e6 / t_plain, "served_mpix_s": px.sum() / 1e6 / t_served,
+                        "plain_req_s": mu, "ratio": t_plain / t_served},
+           "rates": rates,
+           "server": {"batches": st["batches"], "kernel_launches": st["kernel_launches"],
+                      "peak_admitted_gb": st["peak_admitted_bytes"] / 2 ** 30, "peak_inflight": st["peak_inflight"]}}
+    del scenes, outs
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_serving(args):
+    import torch
+
+    import despeckcl_b200 as dcl
+    from despeckcl_b200 import synthetic
+
+    torch.cuda.set_device(0)
+    stats = make_stats(dcl, synthetic)
+    n = args.requests
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        r = serving_measure(args, stats, n, (0.5, 0.8, 1.1))
     line = {
         "metric": "NL-SAR served Mpix/s (Poisson arrivals at 1.1x the plain request rate)",
-        "value": top["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 3,
+        "value": r["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 3,
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (generated on the device, seed = request id)",
-        "config": {"workload": f"{n} requests per stream, sides uniform in [256, 4096], "
-                               f"{px.sum() / 1e6:.0f} Mpix per stream",
-                   "search_window": SWS, "patches": PATCHES, "scales": SCALES, "select_mode": args.mode,
-                   "hbm_budget_gb": args.hbm_budget_gb, "max_inflight": 2, "max_batch_tiles": 148 * 8},
-        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
-        "capacity": {"plain_mpix_s": px.sum() / 1e6 / t_plain, "served_mpix_s": px.sum() / 1e6 / t_served,
-                     "plain_req_s": mu, "ratio": t_plain / t_served},
-        "rates": rates,
-        "server": {"batches": st["batches"], "kernel_launches": st["kernel_launches"],
-                   "peak_admitted_gb": st["peak_admitted_bytes"] / 2 ** 30, "peak_inflight": st["peak_inflight"]},
-        "gpu_launches": st["kernel_launches"], "clocks": clk.summary(),
+        "config": {"workload": r["workload"], "search_window": SWS, "patches": PATCHES, "scales": SCALES,
+                   "select_mode": args.mode, "hbm_budget_gb": args.hbm_budget_gb, "max_inflight": 2,
+                   "max_batch_tiles": 148 * 8},
+        "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "capacity": r["capacity"], "rates": r["rates"],
+        "server": r["server"], "gpu_launches": r["server"]["kernel_launches"], "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0

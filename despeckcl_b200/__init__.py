@@ -28,6 +28,7 @@ from .api import (  # noqa: F401
     nlsar_train_insar,
     store_nlsar_stats_collection,
     stats_from_dissims,
+    take_stage_timeouts,
 )
 
 __version__ = "0.1.0"

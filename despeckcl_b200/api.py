@@ -118,6 +118,16 @@ def _check(rc: int) -> None:
         raise DespeckclError(rc, lib().dcl_last_error().decode(errors="replace"))
 
 
+def take_stage_timeouts() -> int:
+    """Thread blocks of the NL-SAR kernels on the current device that gave up
+    waiting for a TMA staging copy since the last call (their tiles are
+    unwritten); reads and resets the device's ledger.  Call it after
+    synchronising the streams whose launches it should cover."""
+    n = ctypes.c_int(0)
+    _check(lib().dcl_take_stage_timeouts(ctypes.byref(n)))
+    return n.value
+
+
 # ---------------------------------------------------------------------------
 # statistics collections (std::map<nlsar::params, nlsar::stats>)
 # ---------------------------------------------------------------------------

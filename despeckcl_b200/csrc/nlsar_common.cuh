@@ -80,6 +80,13 @@ struct FilterParams {
   PassParams pass[kMaxPasses];
   ComboParams combo[kMaxCombos];
   const float* wtab;  // [ncombo][kMaxLut] composite weights (device)
+  // Staging timeouts of the specialised kernel: a thread block that gives up
+  // waiting for a TMA staging copy leaves its remaining tiles unwritten and is
+  // counted in the device-wide ledger (dcl_take_stage_timeouts) and, where
+  // `timeouts` is set, in that per-launch device word too.
+  int* timeouts;
+  int stage_polls;     // poll limit of a staging wait; 0: the default
+  int withhold_staging;  // tests only: arm the staging barrier without issuing the copies
 };
 
 struct GaussArg {
@@ -157,8 +164,9 @@ __host__ __device__ inline FastStage fast_stage(int wsh, int phm, int tile_h) {
 // configurations; fast_kernel_supported() tells whether `F` has one (for
 // 8-plane covariance input when `full8`).
 bool fast_kernel_supported(const FilterParams& F, bool full8);
-// CTAs of the specialised kernel that gave up waiting for a staging copy
-// since the last call (the count is reset); 0 on success, -1 on a CUDA error
+// Thread blocks of the specialised kernel that gave up waiting for a staging
+// copy on the current device since the last take (read and reset in one
+// atomic exchange); 0 on success, -1 on a CUDA error
 int take_stage_timeouts(int* count);
 cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st,
                               int variant = 0, bool full8 = false);

@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "dcl_internal.h"
 #include "nlsar_common.cuh"
@@ -134,18 +135,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Staging waits are bounded: a copy that has not landed after this many
 // polls (each a hardware-bounded suspension) is reported, not waited for.
+// The thread block then returns: its remaining tiles stay unwritten, and a
+// copy that never landed may still be pending towards its shared memory (the
+// wait ran out only because that copy did not complete).
 constexpr int kStageWaitPolls = 1 << 22;
-__device__ int g_stage_timeouts;  // CTAs that gave up waiting for a staging copy
+__device__ int g_stage_timeouts;  // thread blocks that gave up waiting for a staging copy (device ledger)
+__device__ int g_stage_taken;     // the ledger's value at the last take
 
 // Waits for phase `parity` of `bar` on every thread; false (for every thread
-// of the CTA) when any thread gave up.
-__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity) {
+// of the CTA) when any thread gave up, which is then counted in the device
+// ledger and in the launch's own word (P.timeouts) where it has one.
+__device__ __forceinline__ bool stage_wait(const FilterParams& P, uint64_t* bar, uint32_t parity) {
+  const int polls = P.stage_polls > 0 ? P.stage_polls : kStageWaitPolls;
   bool ok = false;
-  for (int i = 0; i < kStageWaitPolls && !ok; ++i) ok = mbar_try_wait(bar, parity);
+  for (int i = 0; i < polls && !ok; ++i) ok = mbar_try_wait(bar, parity);
   const bool failed = __syncthreads_or(!ok) != 0;
-  if (failed && threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1);
+  if (failed && threadIdx.x == 0) {
+    atomicAdd(&g_stage_timeouts, 1);
+    if (P.timeouts) atomicAdd(P.timeouts, 1);
+  }
   return !failed;
 }
+
+__global__ void take_stage_timeouts_kernel() { g_stage_taken = atomicExch(&g_stage_timeouts, 0); }
 
 // ln det of a staged scaled covariance, rounded like the prep kernel's
 // (sim_measures.h:31-34)
@@ -482,11 +494,13 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(bar, (FULL8 ? 2 : 1) * L::CO_BYTES + L::CS_BYTES);
-      tma_load_2d(sCo, &S.tm_co, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
-      if (FULL8) tma_load_2d(sCo2, &S.tm_co2, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
-      tma_load_2d(sCs, &S.tm_cs[P.pass[0].scale_slot], 4 * (vx0 - PHX - WSH + G), vy0 - PHX - WSH + G, bar);
+      if (!P.withhold_staging) {
+        tma_load_2d(sCo, &S.tm_co, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
+        if (FULL8) tma_load_2d(sCo2, &S.tm_co2, 4 * (vx0 - WSH + G), vy0 - WSH + G, bar);
+        tma_load_2d(sCs, &S.tm_cs[P.pass[0].scale_slot], 4 * (vx0 - PHX - WSH + G), vy0 - PHX - WSH + G, bar);
+      }
     }
-    if (!stage_wait(bar, parity)) return;
+    if (!stage_wait(P, bar, parity)) return;
     parity ^= 1u;
     for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
 
@@ -512,7 +526,7 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
           mbar_expect_tx(bar, L::CS_BYTES);
           tma_load_2d(sCs, &S.tm_cs[pp.scale_slot], 4 * (vx0 - PHX - WSH + G), vy0 - PHX - WSH + G, bar);
         }
-        if (!stage_wait(bar, parity)) return;
+        if (!stage_wait(P, bar, parity)) return;
         parity ^= 1u;
         for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
         loaded_slot = pp.scale_slot;
@@ -620,16 +634,20 @@ cudaError_t launch_fast_insar(int shape, const FilterParams& F, const SceneDesc*
 
 }  // namespace
 
-// Number of CTAs that gave up waiting for a TMA staging copy since the last
-// call (and resets it).  Their tiles were left unwritten.
+// Number of thread blocks that gave up waiting for a TMA staging copy on the
+// current device since the last take; the ledger is read and reset by one
+// atomic exchange on the device, so no increment is lost, and takes from
+// several host threads are serialised.  Their tiles were left unwritten.
 int take_stage_timeouts(int* count) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
   int n = 0;
-  cudaError_t e = cudaMemcpyFromSymbol(&n, g_stage_timeouts, sizeof n);
-  if (e == cudaSuccess && n != 0) {
-    const int zero = 0;
-    e = cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof zero);
-  }
-  *count = n;
+  take_stage_timeouts_kernel<<<1, 1, 0, cudaStreamPerThread>>>();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyFromSymbolAsync(&n, g_stage_taken, sizeof n, 0, cudaMemcpyDeviceToHost, cudaStreamPerThread);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+  *count = e == cudaSuccess ? n : 0;
   return e == cudaSuccess ? 0 : -1;
 }
 

@@ -145,6 +145,16 @@ int make_plan(int sws, const int* patches, int np, const int* scales, int ns, co
 
   FilterParams& F = pl.P;
   std::memset(&F, 0, sizeof F);
+  // tests only: DESPECKCL_B200_TEST_WITHHOLD_STAGING=1 arms the specialised
+  // kernel's staging barrier without issuing the copies, with a short poll
+  // limit, so that every staging wait runs out and the reporting path runs (no
+  // copy is then pending when a thread block gives up)
+  if (const char* w = std::getenv("DESPECKCL_B200_TEST_WITHHOLD_STAGING")) {
+    if (std::strcmp(w, "1") == 0) {
+      F.withhold_staging = 1;
+      F.stage_polls = 256;
+    }
+  }
   pl.full8 = full8;
   pl.px = full8 ? 2 : 4;
   pl.scales = Sv;
@@ -558,6 +568,8 @@ int host_pipe(int dev, size_t nev, HostPipe*& out) {
   cudaError_t e = cudaSuccess;
   if (!p.h2d) e = cudaStreamCreateWithFlags(&p.h2d, cudaStreamNonBlocking);
   if (e == cudaSuccess && !p.d2h) e = cudaStreamCreateWithFlags(&p.d2h, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !p.h_timeouts)
+    e = cudaHostAlloc(reinterpret_cast<void**>(&p.h_timeouts), sizeof(int), cudaHostAllocDefault);
   while (e == cudaSuccess && p.ev.size() < nev) {
     cudaEvent_t ev;
     e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -630,13 +642,17 @@ static int run_host_banded(const Plan& pl0, const float* const* hin, int nin, fl
   const size_t desc_bytes = (nb * sizeof(SceneDesc) + 255) / 256 * 256;
   const size_t wtab_bytes = pl.wtab.size() * sizeof(float);
   const size_t io_bytes = ((size_t)(nin + nout) * b + 255) / 256 * 256;
+  const size_t wtab_pad = (wtab_bytes + 255) / 256 * 256;
   char* mem = nullptr;
-  cudaError_t e = cudaMallocAsync(&mem, io_bytes + scratch + desc_bytes + wtab_bytes, st);
+  // ... + one word: this call's count of thread blocks whose staging wait ran out
+  cudaError_t e = cudaMallocAsync(&mem, io_bytes + scratch + desc_bytes + wtab_pad + 256, st);
   if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(io + scratch)");
   float* buf = reinterpret_cast<float*>(mem);  // [nin][H][W] inputs, then [nout][H][W] outputs
   float* dout = buf + (size_t)nin * n;
   SceneDesc* d_desc = reinterpret_cast<SceneDesc*>(mem + io_bytes + scratch);
   float* d_wtab = reinterpret_cast<float*>(mem + io_bytes + scratch + desc_bytes);
+  int* d_timeouts = reinterpret_cast<int*>(mem + io_bytes + scratch + desc_bytes + wtab_pad);
+  *hp->h_timeouts = 0;
 
   // band b covers tile rows [tb[b], tb[b+1])
   std::vector<int> tb(nb + 1);
@@ -659,12 +675,14 @@ static int run_host_banded(const Plan& pl0, const float* const* hin, int nin, fl
   if (rc == DCL_OK) {
     e = cudaMemcpyAsync(d_desc, desc.data(), nb * sizeof(SceneDesc), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_wtab, pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_timeouts, 0, sizeof(int), st);
     if (e == cudaSuccess) e = cudaEventRecord(ev_alloc, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(hp->h2d, ev_alloc, 0);
     if (e != cudaSuccess) rc = cuda_error(e, "NL-SAR parameters");
   }
   pl.P.wtab = d_wtab;
   pl.P.n_scenes = 1;
+  pl.P.timeouts = d_timeouts;
 
   const int TH = pl.P.tile_h, G = pl.P.G;
   int in_done = 0, co_done = 0, cs_done = 0;
@@ -724,14 +742,17 @@ static int run_host_banded(const Plan& pl0, const float* const* hin, int nin, fl
     cudaStreamSynchronize(hp->h2d);
     cudaStreamSynchronize(hp->d2h);
   }
+  if (rc == DCL_OK) {
+    e2 = cudaMemcpyAsync(hp->h_timeouts, d_timeouts, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR timeout count");
+  }
   cudaFreeAsync(mem, st);
   e2 = cudaStreamSynchronize(st);
   if (rc == DCL_OK && e2 != cudaSuccess) rc = cuda_error(e2, "NL-SAR");
-  if (rc == DCL_OK && uses_specialised_kernel(pl)) {
-    int timeouts = 0;
-    if (take_stage_timeouts(&timeouts) != 0 || timeouts != 0)
-      rc = set_error(DCL_ERR_CUDA, "NL-SAR: %d tiles gave up waiting for their TMA staging copies", timeouts);
-  }
+  if (rc == DCL_OK && *hp->h_timeouts != 0)
+    rc = set_error(DCL_ERR_TIMEOUT,
+                   "NL-SAR: %d thread blocks gave up waiting for their TMA staging copies; their tiles are unwritten",
+                   *hp->h_timeouts);
   return rc;
 }
 
@@ -766,6 +787,16 @@ using namespace dcl;
 extern "C" const char* dcl_last_error(void) { return last_error(); }
 
 extern "C" const char* dcl_version(void) { return "despeckcl_b200 0.1 (sm_100a)"; }
+
+extern "C" int dcl_take_stage_timeouts(int* count) {
+  if (!count) return set_error(DCL_ERR_INVALID_ARGUMENT, "null count");
+  *count = 0;
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_error(e, "no CUDA device");
+  if (take_stage_timeouts(count) != 0) return set_error(DCL_ERR_CUDA, "reading the staging-timeout ledger failed");
+  return DCL_OK;
+}
 
 extern "C" void dcl_profile_begin(void) {
   for (auto& p : g_prof.ev) {

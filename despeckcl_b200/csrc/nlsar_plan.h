@@ -51,6 +51,7 @@ bool uses_specialised_kernel(const Plan& pl);
 struct HostPipe {
   cudaStream_t h2d = nullptr, d2h = nullptr;
   std::vector<cudaEvent_t> ev;
+  int* h_timeouts = nullptr;  // pinned: the last call's staging-timeout count
 };
 int host_pipe(int dev, size_t nev, HostPipe*& out);
 // Row bands of a host-pointer call over `tiles` tiles in `tile_rows` rows

@@ -121,6 +121,8 @@ struct Slot {
   cudaEvent_t prep_done = nullptr, done = nullptr;
   SceneDesc* h_desc = nullptr;  // pinned
   SceneDesc* d_desc = nullptr;
+  int* d_timeouts = nullptr;    // the launch's count of thread blocks whose staging wait ran out
+  int* h_timeouts = nullptr;    // pinned copy, read when the launch has completed
   bool busy = false;
 };
 
@@ -211,12 +213,18 @@ bool dcl_server::retire_locked() {
     const double t = now();
     std::string msg;
     if (q != cudaSuccess) msg = std::string("NL-SAR launch failed: ") + cudaGetErrorString(q);
+    const int timeouts = q == cudaSuccess ? *s.h_timeouts : 0;
+    if (timeouts)
+      msg = "NL-SAR: " + std::to_string(timeouts) +
+            " thread blocks gave up waiting for their TMA staging copies; their tiles are unwritten";
     for (auto& rp : b->reqs) {
       Request* r = rp.get();
       r->open.erase(std::remove(r->open.begin(), r->open.end(), b), r->open.end());
       if (r->prep_batch == b) r->prep_batch = nullptr;
       if (q != cudaSuccess)
         finish_locked(r, DCL_ERR_CUDA, msg, t);
+      else if (timeouts)
+        finish_locked(r, DCL_ERR_TIMEOUT, msg, t);
       else if (r->open.empty() && r->next_tile == r->tiles)
         finish_locked(r, DCL_OK, "", t);
       release_locked(r);
@@ -322,9 +330,14 @@ int dcl_server::enqueue(Batch& b, const std::vector<std::pair<Request*, int>>& p
   F.wtab = d_wtab;
   F.n_scenes = (int)parts.size();
   F.total_tiles = tb;
+  F.timeouts = s.d_timeouts;
+  e = cudaMemsetAsync(s.d_timeouts, 0, sizeof(int), str);
+  if (e != cudaSuccess) return cuda_error(e, "server timeout word");
   int rc = launch_fused(pl, F, s.d_desc, smem, str, variant);
   if (rc) return rc;
   launches += 1;
+  e = cudaMemcpyAsync(s.h_timeouts, s.d_timeouts, sizeof(int), cudaMemcpyDeviceToHost, str);
+  if (e != cudaSuccess) return cuda_error(e, "server timeout word");
   // results of host requests whose last tiles run here
   for (auto& pr : parts) {
     Request* r = pr.first;
@@ -436,6 +449,7 @@ void destroy_server(dcl_server* s) {
     if (sl.prep_done) cudaEventDestroy(sl.prep_done);
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.h_desc) cudaFreeHost(sl.h_desc);
+    if (sl.h_timeouts) cudaFreeHost(sl.h_timeouts);
     if (sl.stream) cudaStreamDestroy(sl.stream);
   }
   if (s->arena_base) cudaFree(s->arena_base);
@@ -474,7 +488,8 @@ extern "C" dcl_server* dcl_server_create(int sws, const int* patches, int np, co
     set_error(DCL_ERR_INVALID_ARGUMENT, "HBM budget too small");
     return nullptr;
   }
-  e = cudaMalloc(&s->arena_base, budget + wtab_bytes + max_inflight * align_up(kMaxScenesPerLaunch * sizeof(SceneDesc)));
+  e = cudaMalloc(&s->arena_base, budget + wtab_bytes +
+                                      max_inflight * (align_up(kMaxScenesPerLaunch * sizeof(SceneDesc)) + kAlign));
   if (e != cudaSuccess) {
     cuda_error(e, "cudaMalloc(server arena)");
     return nullptr;
@@ -488,10 +503,14 @@ extern "C" dcl_server* dcl_server_create(int sws, const int* patches, int np, co
     Slot& sl = s->slots[i];
     sl.d_desc = reinterpret_cast<SceneDesc*>(dp);
     dp += align_up(kMaxScenesPerLaunch * sizeof(SceneDesc));
+    sl.d_timeouts = reinterpret_cast<int*>(dp);
+    dp += kAlign;
     e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.prep_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaHostAlloc(&sl.h_desc, kMaxScenesPerLaunch * sizeof(SceneDesc), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&sl.h_timeouts), sizeof(int), cudaHostAllocDefault);
+    if (e == cudaSuccess) *sl.h_timeouts = 0;
   }
   if (e != cudaSuccess) {
     cuda_error(e, "server set-up");

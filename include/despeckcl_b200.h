@@ -24,6 +24,20 @@
  *                                                                          src/compute/nlinsar/nlinsar.cpp:42-130
  *   dcl_stats_entry          nlsar::params + nlsar::stats                include/compute/nlsar/parameters.h:26-57,
  *                                                                          include/compute/nlsar/stats.h:28-55
+ *
+ * Staging timeouts.  The specialised NL-SAR kernel stages each tile with TMA
+ * copies and waits for them with a bounded wait.  A thread block whose wait
+ * runs out stops and leaves its remaining tiles unwritten (the reference has no
+ * such case: it terminates the process on any OpenCL error,
+ * src/compute/nlsar/nlsar_filter_sub_image.cpp:74-78).  It is reported:
+ *   - by the host-pointer entry points (dcl_nlsar_insar, dcl_nlsar_covmat):
+ *     DCL_ERR_TIMEOUT for that call;
+ *   - by the request server: the requests of the affected launch finish with
+ *     info.status DCL_ERR_TIMEOUT;
+ *   - for every launch, whichever entry point made it: in the device's ledger,
+ *     which dcl_take_stage_timeouts reads and resets.  The device, batched,
+ *     prepared-batch and allocation-free entry points return once their work is
+ *     queued, so their callers read the ledger after synchronising.
  */
 #ifndef DESPECKCL_B200_H
 #define DESPECKCL_B200_H
@@ -69,6 +83,13 @@ typedef struct dcl_stats_collection dcl_stats_collection;
 const char* dcl_last_error(void);
 const char* dcl_version(void);
 
+/* Thread blocks of this library's NL-SAR kernels on the current device that
+ * gave up waiting for a TMA staging copy since the last call (see "Staging
+ * timeouts" above); the ledger is read and reset atomically.  Call it after
+ * synchronising the streams whose launches it should cover.  No reference
+ * counterpart. */
+int dcl_take_stage_timeouts(int* count);
+
 /* Timing of this library's kernels on the calling thread (no reference
  * counterpart; the reference's timed_run, src/clcfg/clcfg.h:97-119, measures
  * host wall clock).  Between begin and end, CUDA events are recorded on the
@@ -91,7 +112,8 @@ int dcl_nlsar_insar(const float* ampl_master, const float* ampl_slave, const flo
 
 /* Same on device pointers, asynchronous on `stream`.  selection_out (device,
  * height x width int32, may be NULL) receives the selected combination's index
- * in the reference loop order (scale outer, patch inner).  Replaces
+ * in the reference loop order (scale outer, patch inner).  A staging timeout
+ * is counted in the device ledger (dcl_take_stage_timeouts).  Replaces
  * despeckcl::nlsar (include/despeckcl.h:45-59). */
 int dcl_nlsar_insar_device(const float* ampl_master, const float* ampl_slave, const float* phase, float* ref_filt,
                            float* phase_filt, float* coh_filt, int height, int width, int search_window_size,
@@ -108,7 +130,10 @@ int dcl_nlsar_insar_device(const float* ampl_master, const float* ampl_slave, co
  * frame does not fit are rejected with DCL_ERR_INVALID_ARGUMENT (about
  * 1000 x 1000 pixels with search 21, patches {3,5,7}, scales {1,3}), and calls
  * that overlap on the GPU race.  The first call on a device resolves the
- * array's address: make it before any stream capture. */
+ * array's address: make it before any stream capture.  The call copies its
+ * scene descriptor and weight tables from pageable host memory, so it may wait
+ * for the stream's earlier work before returning.  A staging timeout is counted
+ * in the device ledger (dcl_take_stage_timeouts). */
 int dcl_nlsar_insar_device_noalloc(const float* ampl_master, const float* ampl_slave, const float* phase,
                                    float* ref_filt, float* phase_filt, float* coh_filt, int height, int width,
                                    int search_window_size, const int* patch_sizes, int n_patch_sizes,
@@ -125,7 +150,9 @@ int dcl_nlsar_covmat(const float* covmat_raw, float* covmat_filt, int height, in
                      int n_scale_sizes, const dcl_stats_entry* stats, int n_stats, float h_param, float c_param,
                      int select_mode);
 
-/* Same on device pointers.  Replaces despeckcl::nlsar (include/despeckcl.h:62-73). */
+/* Same on device pointers, asynchronous on `stream`; a staging timeout is
+ * counted in the device ledger (dcl_take_stage_timeouts).  Replaces
+ * despeckcl::nlsar (include/despeckcl.h:62-73). */
 int dcl_nlsar_covmat_device(const float* covmat_raw, float* covmat_filt, int height, int width, int dim,
                             int search_window_size, const int* patch_sizes, int n_patch_sizes,
                             const int* scale_sizes, int n_scale_sizes, const dcl_stats_entry* stats, int n_stats,
@@ -133,7 +160,8 @@ int dcl_nlsar_covmat_device(const float* covmat_raw, float* covmat_filt, int hei
 
 /* Batched NL-SAR: n_scenes InSAR pairs of possibly different sizes, all
  * filtered with the same parameters in one persistent launch.  Each array
- * holds n_scenes device pointers / sizes.  The batched counterpart of
+ * holds n_scenes device pointers / sizes; a staging timeout is counted in the
+ * device ledger (dcl_take_stage_timeouts).  The batched counterpart of
  * despeckcl::nlsar (include/despeckcl.h:45-59). */
 int dcl_nlsar_insar_batch_device(int n_scenes, const float* const* ampl_master, const float* const* ampl_slave,
                                  const float* const* phase, float* const* ref_filt, float* const* phase_filt,
@@ -150,7 +178,8 @@ int dcl_nlsar_insar_batch_device(int n_scenes, const float* const* ampl_master, 
  * specialised kernel's instantiations on the batch at creation and keeps the
  * fastest (cached per device and configuration; DESPECKCL_B200_TUNE_CACHE names
  * a file that keeps the choices across processes); DCL_BATCH_VARIANT1 selects
- * the 4-pixels-per-thread instantiation without timing.  The batched counterpart of
+ * the 4-pixels-per-thread instantiation without timing.  A run's staging
+ * timeouts are counted in the device ledger (dcl_take_stage_timeouts).  The batched counterpart of
  * despeckcl::nlsar (include/despeckcl.h:45-59); the reference filters one scene
  * per call. */
 enum dcl_batch_flags { DCL_BATCH_GRAPH = 1, DCL_BATCH_AUTOTUNE = 2, DCL_BATCH_VARIANT1 = 4 };
@@ -177,7 +206,8 @@ void dcl_nlsar_batch_destroy(dcl_nlsar_batch* batch);
  * tiles (large scenes are split over several launches, scenes that arrive while
  * one runs join the next), and keeps up to max_inflight launches queued on
  * separate streams.  Results are bitwise those of dcl_nlsar_insar_device on the
- * same scene.  flags: DCL_BATCH_VARIANT1 as for prepared batches. */
+ * same scene.  A launch with a staging timeout fails its requests with
+ * DCL_ERR_TIMEOUT.  flags: DCL_BATCH_VARIANT1 as for prepared batches. */
 typedef struct dcl_server dcl_server;
 typedef struct {
   int status;                  /* DCL_OK, or the error that failed the request */

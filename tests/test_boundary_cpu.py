@@ -161,3 +161,18 @@ int main() {
                     "-ldespeckcl_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True, text=True, check=True).stdout
     assert out.split() == ["1", "256", "99"]
+
+
+def test_stage_timeout_ledger_fails_loudly_without_a_device():
+    # dcl_take_stage_timeouts: a null count is an argument error; without a
+    # CUDA device the ledger cannot be read and the call says so (count 0)
+    L = dcl.lib()
+    assert L.dcl_take_stage_timeouts(None) == -1
+    n = ctypes.c_int(7)
+    rc = L.dcl_take_stage_timeouts(ctypes.byref(n))
+    if rc == 0:
+        pytest.skip("a CUDA device is present")
+    assert rc == -4 and n.value == 0
+    assert "CUDA" in L.dcl_last_error().decode() or "device" in L.dcl_last_error().decode()
+    with pytest.raises(dcl.DespeckclError):
+        dcl.take_stage_timeouts()

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 import despeckcl_b200 as dcl  # noqa: E402
 from despeckcl_b200 import synthetic  # noqa: E402
-from nlsar_parity import KAPPA_MAX, PHASE_TOL, REL_TOL, check_parity, run_gpu, wrapped  # noqa: E402,F401
+from nlsar_parity import KAPPA_MAX, PHASE_TOL, REL_TOL, check_crops, check_parity, run_gpu, wrapped  # noqa: E402,F401
 
 SWS, PATCHES, SCALES = 21, [3, 5, 7], [1, 3]
 
@@ -137,9 +137,16 @@ def test_covariance_path_matches_oracle(oracle, train_stats):
         gi = np.empty_like(o)
         gi[0::2] = g.real.reshape(4, 40, 56)
         gi[1::2] = g.imag.reshape(4, 40, 56)
-        scale = np.maximum(np.abs(o), np.abs(o[[0, 0, 0, 0, 6, 6, 6, 6]]) * 1e-2)
+        # each element within 1e-4 of its own magnitude, or of 1e-2 of the
+        # pixel's larger diagonal where it is much smaller than that (noise on
+        # the imaginary diagonal, near-zero off-diagonals): FP32 rounding of a
+        # weighted sum scales with the magnitudes summed; no scale is zero
+        diag_mag = np.maximum(np.abs(o[0]), np.abs(o[6]))
+        scale = np.maximum(np.abs(o), 1e-2 * diag_mag[None])
+        assert (scale > 0).all()
         err = np.abs(gi - o) / scale
-        assert (err <= 1e-3).mean() >= 0.99, err.max()
+        assert np.isfinite(err).all()
+        assert (err <= 1e-4).mean() >= 0.99, err.max()
 
 
 def test_specialised_and_generic_kernels_agree(tmp_path, train_stats):
@@ -341,14 +348,36 @@ def test_constant_scene_is_a_fixed_point(train_stats):
     np.testing.assert_allclose(coh, 1.0, rtol=1e-5)
 
 
-def test_config1_scene_reference_mode(oracle, train_stats):
-    # the 512 x 512 scene of the first benchmark configuration, seed 1
+@pytest.mark.parametrize("mode", ["reference", "argmax_enl"])
+def test_config1_scene(oracle, train_stats, mode):
+    # the 512 x 512 scene of the first benchmark configuration, seed 1, in
+    # both selection modes (the benchmark runs the ENL argmax)
     a1, a2, ph = synthetic.insar_scene(512, 512, 1)
-    o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=0, use_double=True,
+    m = 0 if mode == "reference" else 1
+    o = oracle.nlsar_insar(a1, a2, ph, SWS, PATCHES, SCALES, train_stats, select_mode=m, use_double=True,
                            diag=True)
-    g = run_gpu(a1, a2, ph, train_stats, "reference")
-    frac_ok, frac_stable = check_parity(g, o[:3], o[3], "reference")
-    print(f"config-1 reference mode: {frac_ok:.5f} within tolerance, {frac_stable:.3f} well conditioned")
+    g = run_gpu(a1, a2, ph, train_stats, mode, selection=True)
+    frac_ok, frac_stable = check_parity(g, o[:3], o[3], mode)
+    d = o[3]
+    clear = ((d.enl_margin > 1e-4) & (d.var_cond > 1e-4) & (d.bin_margin_all > 1e-3)
+             if m == 1 else np.ones(a1.shape, bool))
+    assert np.array_equal(g[3][clear], d.sel[clear])
+    assert (g[3] == d.sel).mean() >= 0.995
+    print(f"config-1 {mode}: {frac_ok:.5f} within tolerance, {frac_stable:.3f} well conditioned")
+
+
+def test_config2_scene_crops_argmax(oracle, train_stats):
+    # the 4096 x 4096 scene of the headline benchmark (seed 1), ENL argmax:
+    # the GPU filters the whole scene, the FP64 oracle six 96 x 96 crops
+    a1, a2, ph = synthetic.insar_scene(4096, 4096, 1)
+    sel = torch.zeros((4096, 4096), dtype=torch.int32, device="cuda")
+    t = [torch.from_numpy(x).cuda() for x in (a1, a2, ph)]
+    out = dcl.nlsar_insar_device(*t, SWS, PATCHES, SCALES, train_stats, select_mode="argmax_enl", selection=sel)
+    torch.cuda.synchronize()
+    g = [x.cpu().numpy() for x in out]
+    frac_ok, frac_stable = check_crops(oracle, train_stats, (a1, a2, ph), g, sel.cpu().numpy(), "argmax_enl",
+                                       ncrops=6, seed=2)
+    print(f"config-2 crops: {frac_ok:.5f} within tolerance, {frac_stable:.3f} well conditioned")
 
 
 def test_boxcar_matches_oracle(oracle):
