@@ -438,7 +438,7 @@ class NlsarBatch:
         pk, pp, npn = _ints(patch_sizes)
         sk, sp, nsn = _ints(scale_sizes)
         arr, ns, keep = _entries(nlsar_stats)
-        flags = (1 if graph else 0) | (2 if autotune else 0) | (4 if variant == 1 else 0)
+        flags = (1 if graph else 0) | (2 if autotune else 0) | (4 if variant == 1 else 0) | (8 if variant == 2 else 0)
         h_ = lib().dcl_nlsar_batch_create(n, *args, hs, ws, int(search_window_size), pp, npn, sp, nsn, arr, ns,
                                           ctypes.c_float(h), ctypes.c_float(c), _mode(select_mode), flags,
                                           _stream(stream))

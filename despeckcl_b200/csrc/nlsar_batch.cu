@@ -28,6 +28,8 @@ struct dcl_nlsar_batch {
   std::vector<dcl::SceneGeom> geo;
   std::vector<dcl::SceneDesc> desc;
   std::vector<const float*> a1, a2, phi;
+  std::vector<float*> ref, phase, coh;
+  std::vector<int> H, W;
   char* scratch = nullptr;
   dcl::SceneDesc* d_desc = nullptr;
   size_t smem = 0;
@@ -40,6 +42,49 @@ struct dcl_nlsar_batch {
 
 namespace dcl {
 namespace {
+
+// Geometry, frames and descriptors of every scene for tiles of `tile_h` rows,
+// carved from the batch's scratch (sized for the tallest tiles; a frame of
+// shorter tiles is never larger), descriptors uploaded synchronously.
+int prepare(dcl_nlsar_batch* b, int tile_h, size_t* scratch_total) {
+  b->pl.P.tile_h = tile_h;
+  const int n = (int)b->H.size();
+  b->geo.clear();
+  std::vector<size_t> offs;
+  size_t total = 0;
+  long long tiles = 0;
+  for (int i = 0; i < n; ++i) {
+    b->geo.push_back(scene_geom(b->pl, b->H[i], b->W[i]));
+    offs.push_back(total);
+    total += (scratch_bytes(b->pl, b->geo.back()) + 255) / 256 * 256;
+    tiles += (long long)b->geo.back().tiles_x * b->geo.back().tiles_y;
+  }
+  if (tiles > 0x7fffffff) return set_error(DCL_ERR_INVALID_ARGUMENT, "batch too large");
+  if (scratch_total) {  // sizing only
+    *scratch_total = total;
+    return DCL_OK;
+  }
+  b->desc.assign(n, SceneDesc{});
+  int tb = 0;
+  for (int i = 0; i < n; ++i) {
+    SceneDesc& d = b->desc[i];
+    std::memset(&d, 0, sizeof d);
+    const int rc = carve_scene(b->pl, b->geo[i], b->scratch + offs[i], d);
+    if (rc != DCL_OK) return rc;
+    d.ref = b->ref[i];
+    d.phase = b->phase[i];
+    d.coh = b->coh[i];
+    d.tile_begin = tb;
+    tb += b->geo[i].tiles_x * b->geo[i].tiles_y;
+  }
+  const cudaError_t e = cudaMemcpy(b->d_desc, b->desc.data(), n * sizeof(SceneDesc), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMemcpy(batch descriptors)");
+  b->pl.P.total_tiles = (int)tiles;
+  return DCL_OK;
+}
+
+// tile rows of a kernel instantiation (launch_nlsar_fast variants)
+int variant_tile_h(int v) { return v == 2 ? kFastTileHHalf : kFastTileH; }
 
 int enqueue(dcl_nlsar_batch* b, cudaStream_t st) {
   for (size_t i = 0; i < b->desc.size(); ++i) {
@@ -101,9 +146,9 @@ int autotune(dcl_nlsar_batch* b, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_load_locked();
     auto it = g_tune.find(key);
-    if (it != g_tune.end()) {
+    if (it != g_tune.end() && it->second < fast_variants(b->pl.P, false)) {
       b->variant = it->second;
-      return DCL_OK;
+      return b->pl.P.tile_h == variant_tile_h(b->variant) ? DCL_OK : prepare(b, variant_tile_h(b->variant), nullptr);
     }
   }
   float best = 0.f;
@@ -111,9 +156,19 @@ int autotune(dcl_nlsar_batch* b, cudaStream_t st) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int v = 0; v < 2; ++v) {
+  const int nv = fast_variants(b->pl.P, false);
+  for (int v = 0; v < nv; ++v) {
     b->variant = v;
-    int rc = enqueue(b, st);  // warm-up (also sets the kernel's shared-memory attribute)
+    int rc = DCL_OK;
+    if (b->pl.P.tile_h != variant_tile_h(v)) {
+      rc = cudaStreamSynchronize(st) == cudaSuccess ? prepare(b, variant_tile_h(v), nullptr) : DCL_ERR_CUDA;
+      if (rc) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+    }
+    rc = enqueue(b, st);  // warm-up (also sets the kernel's shared-memory attribute)
     if (rc == DCL_OK) {
       cudaEventRecord(e0, st);
       rc = enqueue(b, st);
@@ -140,6 +195,11 @@ int autotune(dcl_nlsar_batch* b, cudaStream_t st) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->variant = best_v;
+  if (b->pl.P.tile_h != variant_tile_h(best_v)) {
+    if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(DCL_ERR_CUDA, "autotune");
+    const int rc = prepare(b, variant_tile_h(best_v), nullptr);
+    if (rc) return rc;
+  }
   b->tuned = true;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = best_v;
@@ -183,22 +243,24 @@ extern "C" dcl_nlsar_batch* dcl_nlsar_batch_create(int n, const float* const* a1
     return nullptr;
   }
   b->pl.P.K = K;
-  std::vector<size_t> offs;
-  size_t total = 0;
-  long long tiles = 0;
   for (int i = 0; i < n; ++i) {
     if (heights[i] < 1 || widths[i] < 1 || !a1[i] || !a2[i] || !phi[i] || !ref[i] || !phase[i] || !coh[i]) {
       set_error(DCL_ERR_INVALID_ARGUMENT, "scene %d: empty or null", i);
       delete b;
       return nullptr;
     }
-    b->geo.push_back(scene_geom(b->pl, heights[i], widths[i]));
-    offs.push_back(total);
-    total += (scratch_bytes(b->pl, b->geo.back()) + 255) / 256 * 256;
-    tiles += (long long)b->geo.back().tiles_x * b->geo.back().tiles_y;
+    b->H.push_back(heights[i]);
+    b->W.push_back(widths[i]);
+    b->a1.push_back(a1[i]);
+    b->a2.push_back(a2[i]);
+    b->phi.push_back(phi[i]);
+    b->ref.push_back(ref[i]);
+    b->phase.push_back(phase[i]);
+    b->coh.push_back(coh[i]);
   }
-  if (tiles > 0x7fffffff) {
-    set_error(DCL_ERR_INVALID_ARGUMENT, "batch too large");
+  // scratch for the tallest tiles the autotuner may try
+  size_t total = 0;
+  if (prepare(b, kFastTileH, &total) != DCL_OK) {
     delete b;
     return nullptr;
   }
@@ -212,36 +274,27 @@ extern "C" dcl_nlsar_batch* dcl_nlsar_batch_create(int n, const float* const* a1
   }
   b->d_desc = reinterpret_cast<SceneDesc*>(b->scratch + total);
   float* d_wtab = reinterpret_cast<float*>(b->scratch + total + desc_bytes);
-  b->desc.resize(n);
-  int tb = 0;
-  for (int i = 0; i < n; ++i) {
-    SceneDesc& d = b->desc[i];
-    std::memset(&d, 0, sizeof d);
-    if (carve_scene(b->pl, b->geo[i], b->scratch + offs[i], d) != DCL_OK) {
-      release(b);
-      return nullptr;
-    }
-    d.ref = ref[i];
-    d.phase = phase[i];
-    d.coh = coh[i];
-    d.tile_begin = tb;
-    tb += b->geo[i].tiles_x * b->geo[i].tiles_y;
-    b->a1.push_back(a1[i]);
-    b->a2.push_back(a2[i]);
-    b->phi.push_back(phi[i]);
+  if (prepare(b, b->pl.P.tile_h, nullptr) != DCL_OK) {
+    release(b);
+    return nullptr;
   }
-  e = cudaMemcpy(b->d_desc, b->desc.data(), n * sizeof(SceneDesc), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_wtab, b->pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice);
+  e = cudaMemcpy(d_wtab, b->pl.wtab.data(), wtab_bytes, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
-    cuda_error(e, "cudaMemcpy(batch descriptors)");
+    cuda_error(e, "cudaMemcpy(batch weight tables)");
     release(b);
     return nullptr;
   }
   b->pl.P.wtab = d_wtab;
   b->pl.P.n_scenes = n;
-  b->pl.P.total_tiles = (int)tiles;
   cudaStream_t st = (cudaStream_t)stream;
   if (flags & DCL_BATCH_VARIANT1) b->variant = 1;
+  if ((flags & DCL_BATCH_VARIANT2) && fast_variants(b->pl.P, false) > 2) {
+    b->variant = 2;
+    if (prepare(b, variant_tile_h(2), nullptr) != DCL_OK) {
+      release(b);
+      return nullptr;
+    }
+  }
   if ((flags & DCL_BATCH_AUTOTUNE) && autotune(b, st) != DCL_OK) {
     release(b);
     return nullptr;

@@ -87,6 +87,9 @@ struct FilterParams {
   int* timeouts;
   int stage_polls;     // poll limit of a staging wait; 0: the default
   int withhold_staging;  // tests only: arm the staging barrier without issuing the copies
+  // arithmetic of the specialised kernel's similarities and sums: 0 the ratio
+  // form (default), 1..4 the alternatives of the precision study (nlsar_fast.cu)
+  int prec;
 };
 
 struct GaussArg {
@@ -141,9 +144,11 @@ __global__ void prep_scale_kernel(const float4* cori, int Hp, int Wp, int pitch,
 cudaError_t launch_nlsar_fused(bool full8, const FilterParams& F, const SceneDesc* d_scenes, size_t smem, int grid,
                                cudaStream_t st);
 
-// Tile rows of the specialised kernel: InSAR input, 8-plane covariance input.
+// Tile rows of the specialised kernel: InSAR input, 8-plane covariance input,
+// and the half-height InSAR tiles the batch autotuner may choose.
 constexpr int kFastTileH = 32;
 constexpr int kFastTileH8 = 24;
+constexpr int kFastTileHHalf = 16;
 
 // Staged regions of the specialised kernel's tile (32 x tile_h outputs), in
 // pixels (width x height): scaled covariance RS x RSH, original covariance
@@ -164,6 +169,8 @@ __host__ __device__ inline FastStage fast_stage(int wsh, int phm, int tile_h) {
 // configurations; fast_kernel_supported() tells whether `F` has one (for
 // 8-plane covariance input when `full8`).
 bool fast_kernel_supported(const FilterParams& F, bool full8);
+// number of instantiations (launch_nlsar_fast variants) the autotuner may time
+int fast_variants(const FilterParams& F, bool full8);
 // Thread blocks of the specialised kernel that gave up waiting for a staging
 // copy on the current device since the last take (read and reset in one
 // atomic exchange); 0 on success, -1 on a CUDA error

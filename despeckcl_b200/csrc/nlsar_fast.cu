@@ -29,6 +29,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cuda_fp16.h>
+
 #include <cstdint>
 #include <mutex>
 
@@ -159,22 +161,75 @@ __device__ __forceinline__ bool stage_wait(const FilterParams& P, uint64_t* bar,
 
 __global__ void take_stage_timeouts_kernel() { g_stage_taken = atomicExch(&g_stage_timeouts, 0); }
 
-// ln det of a staged scaled covariance, rounded like the prep kernel's
-// (sim_measures.h:31-34)
-__device__ __forceinline__ float ln_det(const float4 c) {
-  return logf(__fsub_rn(__fmul_rn(c.x, c.y), __fadd_rn(__fmul_rn(c.z, c.z), __fmul_rn(c.w, c.w))));
+// Arithmetic variants of the similarity and the sums (the precision study;
+// kPrecRatio is the default):
+//   kPrecRatio  the GLR as one base-2 log of the ratio
+//               det(A+B)^2 / (2^4 det A det B) (sim_measures.h:52-64 is the
+//               natural log of that ratio), with 1/(4 det) of every staged
+//               pixel precomputed; the similarities and patch sums are in
+//               log2 units and the weight lookup scales by ln 2.  No large
+//               logs cancel, so the similarity keeps about 1e-7 absolute
+//               accuracy where the log form loses the ulps of ln det (~1e-6)
+//   kPrecLog2   the log form 2 ln det(A+B) - ln det A - ln det B - 4 ln 2 with
+//               the per-pixel ln det staged and an approximate base-2 log
+//   kPrecLogf   the log form with the correctly rounded logf, the reference's
+//               arithmetic
+//   kPrecKahan  kPrecRatio with Kahan-compensated patch sums and accumulators
+//   kPrecHalf   kPrecRatio with every similarity rounded to FP16, as FP16
+//               staging of the similarity map would store it
+enum { kPrecRatio = 0, kPrecLog2 = 1, kPrecLogf = 2, kPrecKahan = 3, kPrecHalf = 4 };
+
+template <int PV>
+__host__ __device__ constexpr bool ratio_form() {
+  return PV == kPrecRatio || PV == kPrecKahan || PV == kPrecHalf;
 }
 
+// det of a staged scaled covariance, rounded like the prep kernel's
+// (sim_measures.h:31-34)
+__device__ __forceinline__ float det_of(const float4 c) {
+  return __fsub_rn(__fmul_rn(c.x, c.y), __fadd_rn(__fmul_rn(c.z, c.z), __fmul_rn(c.w, c.w)));
+}
+
+// The per-pixel term of a staged pixel: ln det (log forms) or 1/(4 det)
+// (ratio form; NaN for a negative det, whose log is NaN, +inf for det 0).
+template <int PV>
+__device__ __forceinline__ float pixel_term(const float4 c) {
+  const float d = det_of(c);
+  if (!ratio_form<PV>()) return logf(d);
+  return d >= 0.0f ? __fdiv_rn(0.25f, fabsf(d)) : __int_as_float(0x7fffffff);
+}
+
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float kahan_add(float s, float x, float& c) {
+  const float y = x - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  return t;
+}
+
+template <int PV>
 __device__ __forceinline__ float glr_sim(const float4 a, float la, const float4 b, float lb, float c2d) {
-  // sim_measures.h:52-64 with nlooks 1 and the per-pixel ln det precomputed:
-  // -(2 d ln 2 + ln det A + ln det B - 2 ln det(A+B)); NaN -> 0.  The two ln det
-  // terms are added first, which makes the value exactly symmetric in (A, B).
+  // sim_measures.h:52-64 with nlooks 1 and the per-pixel terms precomputed;
+  // NaN -> 0.  Each form is exactly symmetric in (A, B), which gives the
+  // mirrored half window the reference's values (copy_symm_weights.cl:56-76).
   const float2 d01 = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
   const float2 d23 = __fadd2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
   const float s00 = d01.x, s11 = d01.y, sre = d23.x, sim = d23.y;
   const float det = (s00 * s11) - (sre * sre + sim * sim);
-  const float t = (la + lb) + c2d;
-  float r = fmaf(2.0f * 0.69314718f, __log2f(det), -t);
+  float r;
+  if (ratio_form<PV>()) {
+    // log2 of det |det| / (16 det A det B): negative (NaN log) when det < 0
+    r = lg2_ftz((det * fabsf(det)) * (la * lb));
+    if (PV == kPrecHalf) r = __half2float(__float2half_rn(r));
+  } else {
+    const float t = (la + lb) + c2d;
+    r = (PV == kPrecLogf) ? 2.0f * logf(det) - t : fmaf(2.0f * 0.69314718f, __log2f(det), -t);
+  }
   if (r != r) r = 0.0f;
   return r;
 }
@@ -197,7 +252,7 @@ struct Best {
 // combinations update the selection state.  The staged scaled covariance
 // carries the halo of the call's largest patch; a pass with smaller patches
 // reads its region CO pixels further in.
-template <class L, int PH0, int PH1, int PH2>
+template <class L, int PH0, int PH1, int PH2, int PV>
 __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParams& pp, float* smem,
                                           Best<L::PX, L::NM>& best) {
   constexpr int WSH = L::WSH, K = L::K, RS = L::RS, RO = L::RO, TW = L::TW, PX = L::PX;
@@ -228,6 +283,7 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
     const int e = (i - j * kMaxLut * L::LUTREP) / L::LUTREP;
     sLut[i] = P.wtab[pp.combo[j] * kMaxLut + e];
   }
+  // patch sums in log2 units (ratio form) are scaled by ln 2 in the lookup
   float inv_span[NP], nbias[NP], lm1[NP], dmax[NP];
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
@@ -236,18 +292,27 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
     nbias[j] = -cp.dmin * inv_span[j];
     lm1[j] = cp.lm1;
     dmax[j] = cp.dmax;
+    if (ratio_form<PV>()) {
+      inv_span[j] *= 0.69314718f;
+      dmax[j] *= 1.44269504f;
+    }
   }
   // this lane's copy of the table of component j
   const float* lut_j[NP];
 #pragma unroll
   for (int j = 0; j < NP; ++j) lut_j[j] = sLut + j * kMaxLut * L::LUTREP + (lane & (L::LUTREP - 1));
   float2 acc[PX / 2][NP][NA];  // .x: pixel 2i, .y: pixel 2i+1
+  constexpr int NKC = PV == kPrecKahan ? NA : 1;  // Kahan compensation terms
+  float2 kc[PX / 2][NP][NKC];
 #pragma unroll
   for (int i = 0; i < PX / 2; ++i)
 #pragma unroll
-    for (int j = 0; j < NP; ++j)
+    for (int j = 0; j < NP; ++j) {
 #pragma unroll
       for (int a = 0; a < NA; ++a) acc[i][j][a] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < NKC; ++a) kc[i][j][a] = make_float2(0.f, 0.f);
+    }
   __syncthreads();
 
   for (int dy = -WSH; dy <= WSH; ++dy) {
@@ -264,7 +329,7 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
         const float la = sLd[ci];
         const int ni = ci + dy * RS + dx0;
 #pragma unroll
-        for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim(a, la, sCs[ni + k], sLd[ni + k], c2d);
+        for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim<PV>(a, la, sCs[ni + k], sLd[ni + k], c2d);
       }
       __syncthreads();
       // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
@@ -292,16 +357,21 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
 #pragma unroll
             for (int o = 0; o < 4; ++o) {
               float h[3] = {0.f, 0.f, 0.f};
-              float ring = s[o + PHM];
+              float ring = s[o + PHM], rc = 0.0f;
 #pragma unroll
               for (int j = 0; j < 3; ++j)
                 if (ph_of<PH0, PH1, PH2>(j) == 0) h[j] = ring;
 #pragma unroll
               for (int b = 1; b <= PHM; ++b) {
-                ring += s[o + PHM - b] + s[o + PHM + b];
+                if (PV == kPrecKahan) {
+                  ring = kahan_add(ring, s[o + PHM - b], rc);
+                  ring = kahan_add(ring, s[o + PHM + b], rc);
+                } else {
+                  ring += s[o + PHM - b] + s[o + PHM + b];
+                }
 #pragma unroll
                 for (int j = 0; j < 3; ++j)
-                  if (ph_of<PH0, PH1, PH2>(j) == b) h[j] = ring;
+                  if (ph_of<PH0, PH1, PH2>(j) == b) h[j] = PV == kPrecKahan ? ring - rc : ring;
               }
 #pragma unroll
               for (int j = 0; j < NP; ++j) hs[j][o] = h[j];
@@ -339,9 +409,15 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
             for (int j = 0; j < NP; ++j) {
               // top-down sum of the 2ph+1 rows (the first term starts the sum:
               // no similarity sum is -0, so this equals 0 + ... bit for bit)
-              float d = hv[j][i];
+              float d = hv[j][i], dc = 0.0f;
 #pragma unroll
-              for (int a = 1; a <= 2 * ph_of<PH0, PH1, PH2>(j); ++a) d += hv[j][i + a];
+              for (int a = 1; a <= 2 * ph_of<PH0, PH1, PH2>(j); ++a) {
+                if (PV == kPrecKahan)
+                  d = kahan_add(d, hv[j][i + a], dc);
+                else
+                  d += hv[j][i + a];
+              }
+              if (PV == kPrecKahan) d -= dc;
               // index = (unsigned)((clamp(d) - dmin) / (dmax - dmin) * (L - 1)):
               // a saturating FMA clamps (and maps NaN to 0), a round-toward-zero
               // add of 2^23 truncates, and the float's low mantissa bits are the
@@ -377,14 +453,29 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
           for (int j = 0; j < NP; ++j) {
             float2* A = acc[i / 2][j];
             const float2 ww = make_float2(w[i][j], w[i + 1][j]);
-            A[0] = __fadd2_rn(A[0], ww);
-            A[1] = __ffma2_rn(ww, ww, A[1]);
-            A[2] = __ffma2_rn(ww, vx, A[2]);
-            A[3] = __ffma2_rn(ww, vy, A[3]);
-            A[4] = __ffma2_rn(ww, x2, A[4]);
-            A[5] = __ffma2_rn(ww, y2, A[5]);
-            A[6] = __ffma2_rn(ww, vz, A[6]);
-            A[7] = __ffma2_rn(ww, vw, A[7]);
+            if (PV == kPrecKahan) {
+              // compensated: y = w v - c, t = A + y, c = (t - A) - y
+              float2* C = kc[i / 2][j];
+              const float2 one = make_float2(1.0f, 1.0f);
+              const float2 terms[8] = {one, ww, vx, vy, x2, y2, vz, vw};
+#pragma unroll
+              for (int e = 0; e < 8; ++e) {
+                const float2 y = __ffma2_rn(ww, terms[e], make_float2(-C[e % NKC].x, -C[e % NKC].y));
+                const float2 t = __fadd2_rn(A[e], y);
+                const float2 u = __fadd2_rn(t, make_float2(-A[e].x, -A[e].y));
+                C[e % NKC] = __fadd2_rn(u, make_float2(-y.x, -y.y));
+                A[e] = t;
+              }
+            } else {
+              A[0] = __fadd2_rn(A[0], ww);
+              A[1] = __ffma2_rn(ww, ww, A[1]);
+              A[2] = __ffma2_rn(ww, vx, A[2]);
+              A[3] = __ffma2_rn(ww, vy, A[3]);
+              A[4] = __ffma2_rn(ww, x2, A[4]);
+              A[5] = __ffma2_rn(ww, y2, A[5]);
+              A[6] = __ffma2_rn(ww, vz, A[6]);
+              A[7] = __ffma2_rn(ww, vw, A[7]);
+            }
             if (FULL8) {
 #pragma unroll
               for (int e = 0; e < 4; ++e) A[(8 + e) % NA] = __ffma2_rn(ww, ex[e], A[(8 + e) % NA]);
@@ -406,7 +497,10 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
     for (int j = 0; j < NP; ++j) {
       float A[NA];
 #pragma unroll
-      for (int a = 0; a < NA; ++a) A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
+      for (int a = 0; a < NA; ++a) {
+        A[a] = (i & 1) ? acc[i / 2][j][a].y : acc[i / 2][j][a].x;
+        if (PV == kPrecKahan && a < NKC) A[a] -= (i & 1) ? kc[i / 2][j][a].y : kc[i / 2][j][a].x;
+      }
       const float s0 = A[0], s1 = A[1], s2 = A[2], s3 = A[3], s4 = A[4], s5 = A[5], s6 = A[6], s7 = A[7];
       const float enl = s0 * s0 / s1;
       const float i0 = s2 / s0, i1 = s3 / s0;
@@ -453,7 +547,7 @@ struct FastK {
   using L = FastL<WSH, PHX, cmax(np_of<A0, A1, A2>(), np_of<B0, B1, B2>()), PX_, TH_, FULL8_>;
 };
 
-template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_>
+template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_, int PV>
 __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
   using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
@@ -502,7 +596,7 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
     }
     if (!stage_wait(P, bar, parity)) return;
     parity ^= 1u;
-    for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
+    for (int i = tid; i < RS * RSH; i += NT) sLd[i] = pixel_term<PV>(sCs[i]);
 
     Best<PX, NM> best;
 #pragma unroll
@@ -528,16 +622,16 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
         }
         if (!stage_wait(P, bar, parity)) return;
         parity ^= 1u;
-        for (int i = tid; i < RS * RSH; i += NT) sLd[i] = ln_det(sCs[i]);
+        for (int i = tid; i < RS * RSH; i += NT) sLd[i] = pixel_term<PV>(sCs[i]);
         loaded_slot = pp.scale_slot;
       }
       if constexpr (B0 < 0) {
-        fast_pass<L, A0, A1, A2>(P, pp, smem, best);
+        fast_pass<L, A0, A1, A2, PV>(P, pp, smem, best);
       } else {
         if (pass_is<A0, A1, A2>(pp))
-          fast_pass<L, A0, A1, A2>(P, pp, smem, best);
+          fast_pass<L, A0, A1, A2, PV>(P, pp, smem, best);
         else
-          fast_pass<L, B0, B1, B2>(P, pp, smem, best);
+          fast_pass<L, B0, B1, B2, PV>(P, pp, smem, best);
       }
     }
 
@@ -584,15 +678,17 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
   }
 }
 
-template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_>
+template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int PX_, int TH_, bool FULL8_,
+          int PV = kPrecRatio>
 cudaError_t launch_fast_t(const FilterParams& F, const SceneDesc* d_scenes, int grid, cudaStream_t st) {
   using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
   const size_t smem = (size_t)L::WORDS * 4;
   static size_t allowed[kMaxDevices];
-  const void* fn = (const void*)nlsar_fast_kernel<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>;
+  const void* fn = (const void*)nlsar_fast_kernel<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_, PV>;
   const cudaError_t e = allow_dynamic_smem(fn, smem, allowed);
   if (e != cudaSuccess) return e;
-  nlsar_fast_kernel<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_><<<grid, L::THREADS, smem, st>>>(F, d_scenes);
+  nlsar_fast_kernel<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_, PV><<<grid, L::THREADS, smem, st>>>(F,
+                                                                                                        d_scenes);
   return cudaGetLastError();
 }
 
@@ -624,6 +720,17 @@ template <int PX_>
 cudaError_t launch_fast_insar(int shape, const FilterParams& F, const SceneDesc* d_scenes, int grid,
                               cudaStream_t st) {
   constexpr int T = kFastTileH;
+  if (shape == 1 && PX_ == 2) {
+    // the arithmetic variants of the precision study (headline shape only)
+    switch (F.prec) {
+      case kPrecLog2: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, T, false, kPrecLog2>(F, d_scenes, grid, st);
+      case kPrecLogf: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, T, false, kPrecLogf>(F, d_scenes, grid, st);
+      case kPrecKahan:
+        return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, T, false, kPrecKahan>(F, d_scenes, grid, st);
+      case kPrecHalf: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, T, false, kPrecHalf>(F, d_scenes, grid, st);
+      default: break;
+    }
+  }
   switch (shape) {
     case 1: return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, PX_, T, false>(F, d_scenes, grid, st);
     case 2: return launch_fast_t<10, 1, 1, -1, -1, -1, -1, -1, PX_, T, false>(F, d_scenes, grid, st);
@@ -658,9 +765,21 @@ int take_stage_timeouts(int* count) {
 // scale, the reference example's settings).
 bool fast_kernel_supported(const FilterParams& F, bool full8) { return fast_shape(F, full8) != 0; }
 
+// Instantiations the batch autotuner may time: 0 and 1 (2 or 4 pixels per
+// thread on 32 x 32 tiles) for InSAR input with patches up to 7, and 2 (32 x 16
+// tiles, 2 pixels per thread, 256-thread CTAs) for the patches {3,5,7} shape;
+// 1 otherwise.  Variant 2 needs the scene geometry of 16-row tiles.
+int fast_variants(const FilterParams& F, bool full8) {
+  const int shape = fast_shape(F, full8);
+  if (full8 || shape == 0 || shape >= 5) return 1;
+  return shape == 1 ? 3 : 2;
+}
+
 // InSAR input (32 x 32 tiles): variant 0 has 2 pixels per thread in
 // 512-thread CTAs (the default), variant 1 4 pixels per thread in 256-thread
-// CTAs (the patch sizes up to 7; the batch autotuner times both).  8-plane
+// CTAs (the patch sizes up to 7), variant 2 32 x 16 tiles with 2 pixels per
+// thread in 256-thread CTAs (patches {3,5,7}; F.tile_h must be 16); the batch
+// autotuner times them (fast_variants).  8-plane
 // covariance input: 32 x 24 tiles, 2 pixels per thread, 384-thread CTAs (the
 // second staged covariance plane and its four accumulators per patch size
 // need the room).
@@ -682,6 +801,8 @@ cudaError_t launch_nlsar_fast(const FilterParams& F, const SceneDesc* d_scenes, 
     case 6: return launch_fast_t<10, 5, 5, -1, -1, -1, -1, -1, 2, T, false>(F, d_scenes, grid, st);
     case 7: return launch_fast_t<10, 5, 1, 2, 3, 4, 5, -1, 2, T, false>(F, d_scenes, grid, st);
     default:
+      if (variant == 2 && shape == 1 && F.tile_h == kFastTileHHalf)
+        return launch_fast_t<10, 3, 1, 2, 3, -1, -1, -1, 2, kFastTileHHalf, false>(F, d_scenes, grid, st);
       if (variant == 1) return launch_fast_insar<4>(shape, F, d_scenes, grid, st);
       return launch_fast_insar<2>(shape, F, d_scenes, grid, st);
   }

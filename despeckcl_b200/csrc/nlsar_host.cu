@@ -149,6 +149,12 @@ int make_plan(int sws, const int* patches, int np, const int* scales, int ns, co
   // kernel's staging barrier without issuing the copies, with a short poll
   // limit, so that every staging wait runs out and the reporting path runs (no
   // copy is then pending when a thread block gives up)
+  // precision study: DESPECKCL_B200_PRECISION=n selects the specialised
+  // kernel's arithmetic variant n (0 default; see nlsar_fast.cu)
+  if (const char* pv = std::getenv("DESPECKCL_B200_PRECISION")) {
+    const int v = std::atoi(pv);
+    if (v >= 0 && v <= 4) F.prec = v;
+  }
   if (const char* w = std::getenv("DESPECKCL_B200_TEST_WITHHOLD_STAGING")) {
     if (std::strcmp(w, "1") == 0) {
       F.withhold_staging = 1;

@@ -177,12 +177,16 @@ int dcl_nlsar_insar_batch_device(int n_scenes, const float* const* ampl_master, 
  * graph (each run is one graph launch); DCL_BATCH_AUTOTUNE times the
  * specialised kernel's instantiations on the batch at creation and keeps the
  * fastest (cached per device and configuration; DESPECKCL_B200_TUNE_CACHE names
- * a file that keeps the choices across processes); DCL_BATCH_VARIANT1 selects
- * the 4-pixels-per-thread instantiation without timing.  A run's staging
+ * a file that keeps the choices across processes).  The autotuner times up to
+ * three tile shapes: 32 x 32 tiles with 2 or 4 pixels per thread (variants 0
+ * and 1) and, for patches {3,5,7}, 32 x 16 tiles with 2 pixels per thread
+ * (variant 2, the batch's frames re-carved for 16-row tiles); every shape
+ * gives the same bits.  DCL_BATCH_VARIANT1 / DCL_BATCH_VARIANT2 select
+ * variant 1 / 2 without timing (variant 2 where the shape has it).  A run's staging
  * timeouts are counted in the device ledger (dcl_take_stage_timeouts).  The batched counterpart of
  * despeckcl::nlsar (include/despeckcl.h:45-59); the reference filters one scene
  * per call. */
-enum dcl_batch_flags { DCL_BATCH_GRAPH = 1, DCL_BATCH_AUTOTUNE = 2, DCL_BATCH_VARIANT1 = 4 };
+enum dcl_batch_flags { DCL_BATCH_GRAPH = 1, DCL_BATCH_AUTOTUNE = 2, DCL_BATCH_VARIANT1 = 4, DCL_BATCH_VARIANT2 = 8 };
 typedef struct dcl_nlsar_batch dcl_nlsar_batch;
 dcl_nlsar_batch* dcl_nlsar_batch_create(int n_scenes, const float* const* ampl_master,
                                         const float* const* ampl_slave, const float* const* phase,
@@ -192,7 +196,8 @@ dcl_nlsar_batch* dcl_nlsar_batch_create(int n_scenes, const float* const* ampl_m
                                         int n_scale_sizes, const dcl_stats_entry* stats, int n_stats,
                                         float h_param, float c_param, int select_mode, int flags, void* stream);
 int dcl_nlsar_batch_run(dcl_nlsar_batch* batch, void* stream);
-/* The kernel instantiation in use (0: 2 pixels per thread, 1: 4). */
+/* The kernel instantiation in use (0: 32 x 32 tiles, 2 pixels per thread;
+ * 1: 32 x 32, 4 pixels per thread; 2: 32 x 16, 2 pixels per thread). */
 int dcl_nlsar_batch_variant(const dcl_nlsar_batch* batch);
 /* Kernels one run launches (prep kernels per scene plus the fused launch). */
 int dcl_nlsar_batch_launches(const dcl_nlsar_batch* batch);

@@ -429,18 +429,19 @@ def test_prepared_batch_graph_autotune_equal_single_scenes(train_stats):
 
 
 def test_kernel_instantiations_agree_bitwise(train_stats):
-    # the 2- and 4-pixel-per-thread instantiations sum in the same per-pixel
-    # order, so they agree exactly
+    # the 2- and 4-pixel-per-thread instantiations on 32 x 32 tiles and the
+    # 32 x 16-tile one sum in the same per-pixel order, so they agree exactly
     a1, a2, ph = synthetic.insar_scene(77, 99, 60)
     tens = [tuple(torch.from_numpy(x).cuda() for x in (a1, a2, ph))]
     res = []
-    for v in (0, 1):
+    for v in (0, 1, 2):
         b = dcl.NlsarBatch(tens, SWS, PATCHES, SCALES, train_stats, graph=False, autotune=False, variant=v)
         assert b.variant == v
         res.append([o.cpu().numpy() for o in b.run()[0]])
         b.close()
-    for a, r in zip(res[0], res[1]):
-        np.testing.assert_array_equal(a, r)
+    for other in res[1:]:
+        for a, r in zip(res[0], other):
+            np.testing.assert_array_equal(a, r)
 
 
 def _polsar_scene(H, W, seed, homogeneous=False):
