@@ -88,7 +88,7 @@ def nlsar_cases():
 
 
 def check_crops(oracle, stats, inputs, gpu, gpu_sel, mode, ncrops=4, crop=96, seed=0, sws=21, patches=(3, 5, 7),
-                scales=(1, 3)):
+                scales=(1, 3), min_stable=0.3):
     """Parity of a whole-scene GPU result on seeded crops: the FP64 oracle
     filters each crop with a margin of `overlap` pixels, so the crop's interior
     sees exactly its neighbourhood in the scene; the interiors are held to
@@ -122,7 +122,11 @@ def check_crops(oracle, stats, inputs, gpu, gpu_sel, mode, ncrops=4, crop=96, se
         setattr(diag, k, np.concatenate([d[k] for d in d_all]))
     g = [cat(g_all, i) for i in range(3)]
     o = [cat(o_all, i) for i in range(3)]
-    frac = check_parity(g, o, diag, mode)
+    # about 43 % of the pixels of the benchmark scenes are well conditioned in
+    # ENL-argmax mode (the 8192 x 8192 precision scene): with 441 weights of the
+    # selected combination, one of them lies within 1e-3 index units of a LUT
+    # bin edge for more than half of the pixels
+    frac = check_parity(g, o, diag, mode, min_stable=min_stable)
     sel = np.concatenate(s_all)
     if m == 1:
         clear = (diag.enl_margin > 1e-4) & (diag.var_cond > 1e-4) & (diag.bin_margin_all > 1e-3)
