@@ -90,12 +90,41 @@ __global__ void __launch_bounds__(kBoxThreads)
   }
 }
 
+// Window sums of 4 consecutive outputs o[q] = v[q] + ... + v[q + w - 1],
+// q = 0..3, from the 4 + w - 1 values v: the part v[3 .. w-1] that all four
+// windows share is added once, then each window adds its own ends (w + 6 adds
+// instead of 4 w).  No term is subtracted, so no sum cancels.
+template <int R>
+__device__ __forceinline__ void window4(const float* v, float* o) {
+  constexpr int w = 2 * R + 1;
+  if (w < 4) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float acc = v[q];
+#pragma unroll
+      for (int k = 1; k < w; ++k) acc += v[q + k];
+      o[q] = acc;
+    }
+    return;
+  }
+  float c = v[3];
+#pragma unroll
+  for (int k = 4; k < w; ++k) c += v[k];
+  const float l1 = v[1] + v[2];
+  const float l0 = v[0] + l1;
+  const float r2 = v[w] + v[w + 1];
+  const float r3 = r2 + v[w + 2];
+  o[0] = l0 + c;
+  o[1] = (l1 + c) + v[w];
+  o[2] = (v[2] + c) + r2;
+  o[3] = c + r3;
+}
+
 // Compile-time window radius R (w = 2R+1 <= 15): a 64 x 32 tile per CTA,
 // window sums from registers, each thread producing 4 consecutive outputs
 // (columns in the horizontal pass, rows in the vertical one) from 4 + 2R
-// loaded values per plane.  Every output sums its window left to right
-// (top to bottom) from 0, as the generic kernel does, so both give the same
-// bits.
+// loaded values per plane, with the shared part of their windows summed once
+// (window4).
 template <int R>
 __global__ void __launch_bounds__(kBoxThreads)
     boxcar_r_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
@@ -150,13 +179,7 @@ __global__ void __launch_bounds__(kBoxThreads)
 #pragma unroll
     for (int k = 0; k < N; ++k) v[k] = src[k];
     float o[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      float acc = 0.f;
-#pragma unroll
-      for (int k = 0; k <= 2 * R; ++k) acc += v[q + k];
-      o[q] = acc;
-    }
+    window4<R>(v, o);
     *reinterpret_cast<float4*>(sHs + pl * SH * kBoxTW + rr * kBoxTW + c0) = make_float4(o[0], o[1], o[2], o[3]);
   }
   __syncthreads();
@@ -171,13 +194,7 @@ __global__ void __launch_bounds__(kBoxThreads)
       float v[N];
 #pragma unroll
       for (int k = 0; k < N; ++k) v[k] = src[k * kBoxTW];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float acc = 0.f;
-#pragma unroll
-        for (int k = 0; k <= 2 * R; ++k) acc += v[q + k];
-        sum[pl][q] = acc;
-      }
+      window4<R>(v, sum[pl]);
     }
     const int vx = vx0 + cc;
     const int ox = (vx < W - 1) ? vx : (vx == W - 1 + R ? W - 1 : -1);

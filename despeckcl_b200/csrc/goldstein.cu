@@ -35,6 +35,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "../../include/despeckcl_b200.h"
@@ -42,6 +43,13 @@
 
 namespace dcl {
 namespace {
+
+// DESPECKCL_B200_GOLDSTEIN_TWO_PASS=1: the two-kernel path (patches through
+// HBM), kept to compare the fused kernel against bit for bit
+const bool g_goldstein_two_pass = [] {
+  const char* v = std::getenv("DESPECKCL_B200_GOLDSTEIN_TWO_PASS");
+  return v && v[0] == '1';
+}();
 
 constexpr int kP = 32;           // patch side (the FFT length)
 constexpr int kWarps = 4;        // patches per CTA (34 KB of transpose buffers)
@@ -279,6 +287,199 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused kernel: patch FFTs and the overlap-add in one launch, no patch scratch
+// in HBM.  A CTA owns a strip of kStripX patch columns and a band of patch
+// rows of the (single) tile.  Its kStripX + 1 warps filter one patch each per
+// patch row (the extra warp the column left of the strip, whose right edge
+// overlaps it), then every thread adds, for the tile rows whose covering
+// patches are all filtered now, the raw interferogram and the weighted patch
+// samples in the reference's parity order and writes |Z| and arg Z.  A tile row
+// is covered by its patch row q and, in its first 2 ov rows, by q - 1: the last
+// 2 ov rows of every filtered patch are kept in shared memory for the next
+// patch row, so each patch is filtered once per strip and band (plus one row
+// and one column of overlap with the neighbouring CTAs).
+// ---------------------------------------------------------------------------
+
+constexpr int kStripX = 7;              // patch columns finalised per CTA
+constexpr int kFusedWarps = kStripX + 1;
+constexpr int kBandRows = 16;           // patch rows finalised per CTA
+constexpr int kMaxOv2 = kP / 2 - 1;     // 2 ov < p / 2
+
+struct GoldsteinBands {
+  int rows_main;   // patch rows 0 .. rows_main - 1 hold tile rows [ov, H + ov - 2]
+  int row_far;     // patch row of tile row sub - ov - 1 when it lies past them, else -1
+  int bands_main;  // ceil(rows_main / kBandRows)
+  int cols_main, col_far, strips_main;  // the same for columns (kStripX per strip)
+};
+
+__device__ __forceinline__ void filter_patch(const float* __restrict__ a1, const float* __restrict__ a2,
+                                             const float* __restrict__ phi, float2* buf, const GoldsteinGeom& g,
+                                             int py, int px, float alpha, int lane) {
+  // gather: lane = column of the patch (the clamp-extended raw interferogram)
+  {
+    const int tx = clampg(px * g.s + lane - g.ov, 0, g.sub - 1);
+    const int ix = clampg(tx - g.ov, 0, g.W - 1);
+#pragma unroll 4
+    for (int r = 0; r < kP; ++r) {
+      const int ty = clampg(py * g.s + r - g.ov, 0, g.sub - 1);
+      const int iy = clampg(ty - g.ov, 0, g.H - 1);
+      const size_t i = (size_t)iy * g.W + ix;
+      const float amp = 0.5f * (a1[i] + a2[i]);
+      float sn, cs;
+      __sincosf(phi[i], &sn, &cs);
+      buf[r * kPitch + lane] = make_float2(amp * cs, amp * sn);
+    }
+  }
+  __syncwarp();
+  float2 x[kP];
+#pragma unroll
+  for (int k = 0; k < kP; ++k) x[k] = buf[lane * kPitch + k];
+  fft32<false>(x);
+#pragma unroll
+  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = x[k];
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < kP; ++r) x[r] = buf[r * kPitch + lane];
+  fft32<false>(x);
+  const float half_alpha = 0.5f * alpha;
+#pragma unroll
+  for (int r = 0; r < kP; ++r) {
+    const float m2 = x[r].x * x[r].x + x[r].y * x[r].y;
+    const float w = (alpha == 0.0f) ? 1.0f : ex2_approx(half_alpha * __log2f(m2));
+    x[r] = make_float2(w * x[r].x, w * x[r].y);
+  }
+  fft32<true>(x);
+#pragma unroll
+  for (int r = 0; r < kP; ++r) buf[r * kPitch + lane] = x[r];
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < kP; ++k) x[k] = buf[lane * kPitch + k];
+  fft32<true>(x);
+  constexpr float kScale = 1.0f / (kP * kP);
+#pragma unroll
+  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = make_float2(x[k].x * kScale, x[k].y * kScale);
+}
+
+// tile position t -> output index (row or column), or -1 when no output
+// takes its value: t = o + ov for o < N - 1, t = sub - ov - 1 for o = N - 1
+__device__ __forceinline__ int out_of_tile(int t, int n_out, const GoldsteinGeom& g) {
+  if (t == g.sub - g.ov - 1) return n_out - 1;
+  const int o = t - g.ov;
+  return (o >= 0 && o < n_out - 1) ? o : -1;
+}
+
+__global__ void __launch_bounds__(32 * kFusedWarps, 2)
+    goldstein_fused_kernel(const float* __restrict__ a1, const float* __restrict__ a2,
+                           const float* __restrict__ phi, float* __restrict__ ref, float* __restrict__ phase,
+                           GoldsteinGeom g, GoldsteinBands B, float alpha) {
+  extern __shared__ float2 gsm[];
+  float2* cur = gsm;                                       // [warps][kP * kPitch]
+  float2* prev = gsm + (size_t)kFusedWarps * kP * kPitch;  // [warps][2 ov][kP]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ov2 = 2 * g.ov;
+  // this CTA's patch columns (finalised: [c0, c1)) and patch rows ([r0, r1))
+  int c0, c1, r0, r1;
+  if ((int)blockIdx.x < B.strips_main) {
+    c0 = blockIdx.x * kStripX;
+    c1 = min(c0 + kStripX, B.cols_main);
+  } else {
+    c0 = B.col_far;
+    c1 = c0 + 1;
+  }
+  if ((int)blockIdx.y < B.bands_main) {
+    r0 = blockIdx.y * kBandRows;
+    r1 = min(r0 + kBandRows, B.rows_main);
+  } else {
+    r0 = B.row_far;
+    r1 = r0 + 1;
+  }
+  const int pxw = c0 - 1 + warp;  // this warp's patch column
+  const bool col_ok = pxw >= 0 && pxw < c1;
+  float2* mycur = cur + (size_t)warp * kP * kPitch;
+  float2* myprev = prev + (size_t)warp * kMaxOv2 * kP;
+  const int tx_lo = c0 * g.s - g.ov, tx_hi = c1 * g.s - g.ov;  // tile columns finalised
+  const int nx = tx_hi - tx_lo;
+  const float inv_nx = 1.0f / (float)nx;
+  for (int q = max(r0 - 1, 0); q < r1; ++q) {
+    if (col_ok) filter_patch(a1, a2, phi, mycur, g, q, pxw, alpha, lane);
+    __syncthreads();
+    if (q >= r0) {
+      // tile rows [q s - ov, (q + 1) s - ov): patch row q at offset ry, and
+      // q - 1 at ry + s for ry < 2 ov
+      const int ty_lo = q * g.s - g.ov;
+      for (int it = threadIdx.x; it < g.s * nx; it += blockDim.x) {
+        // it / nx and cxr / s by a float estimate corrected to the exact
+        // quotient (it < 2^24)
+        int ry = __float2int_rz((float)it * inv_nx);
+        if (ry * nx > it) --ry;
+        if ((ry + 1) * nx <= it) ++ry;
+        const int cxr = it - ry * nx;
+        const int ty = ty_lo + ry, tx = tx_lo + cxr;
+        const int y = out_of_tile(ty, g.H, g), x = out_of_tile(tx, g.W, g);
+        if (y < 0 || x < 0) continue;
+        const size_t i = (size_t)clampg(ty - g.ov, 0, g.H - 1) * g.W + clampg(tx - g.ov, 0, g.W - 1);
+        float2 v;
+        {
+          const float amp = 0.5f * (a1[i] + a2[i]);
+          float sn, cs;
+          __sincosf(phi[i], &sn, &cs);
+          v = make_float2(amp * cs, amp * sn);
+        }
+        // covering patches: row q (offset ry) and q - 1 (offset ry + s);
+        // column qx = (tx + ov) / s (offset cx) and qx - 1 (offset cx + s)
+        const int qx = c0 + div_s(cxr, g), cx = cxr - (qx - c0) * g.s;
+        const bool vy1 = q >= 1 && ry < ov2;
+        const bool vx1 = qx >= 1 && cx < ov2;
+        const bool ye1 = q & 1, xe1 = qx & 1;
+        // index 0: the even patch, 1: the odd one (the reference's parity launches)
+        float fy[2], fx[2];
+        bool vy[2], vx[2];
+        vy[ye1 ? 1 : 0] = true;
+        vy[ye1 ? 0 : 1] = vy1;
+        vx[xe1 ? 1 : 0] = true;
+        vx[xe1 ? 0 : 1] = vx1;
+        fy[ye1 ? 1 : 0] = pack_factor(ry, ty, g.ov, g.sub);
+        fy[ye1 ? 0 : 1] = pack_factor(ry + g.s, ty, g.ov, g.sub);
+        fx[xe1 ? 1 : 0] = pack_factor(cx, tx, g.ov, g.sub);
+        fx[xe1 ? 0 : 1] = pack_factor(cx + g.s, tx, g.ov, g.sub);
+        // warp of patch column qx is qx - c0 + 1; of qx - 1, qx - c0
+        const int wq = qx - c0 + 1;
+#pragma unroll
+        for (int xpar = 0; xpar < 2; ++xpar)
+#pragma unroll
+          for (int ypar = 0; ypar < 2; ++ypar) {
+            if (!vx[xpar] || !vy[ypar]) continue;
+            const bool xcur = (xpar == 1) == xe1;  // the column qx itself
+            const bool ycur = (ypar == 1) == ye1;  // the row q itself
+            const int w = xcur ? wq : wq - 1;
+            const int c = xcur ? cx : cx + g.s;
+            const float2 smp = ycur ? cur[(size_t)w * kP * kPitch + ry * kPitch + c]
+                                    : prev[(size_t)w * kMaxOv2 * kP + ry * kP + c];
+            const float f = fx[xpar] * fy[ypar];
+            v.x += f * smp.x;
+            v.y += f * smp.y;
+          }
+        const size_t o = (size_t)y * g.W + x;
+        ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
+        phase[o] = atan2f(v.y, v.x);
+      }
+    }
+    __syncthreads();
+    // keep the last 2 ov rows of this patch row for the next one
+    if (col_ok)
+      for (int k = lane; k < ov2 * kP; k += 32) {
+        const int r = k / kP, c = k - r * kP;
+        myprev[k] = mycur[(g.s + r) * kPitch + c];
+      }
+    __syncwarp();
+  }
+}
+
+size_t goldstein_fused_smem() {
+  return ((size_t)kFusedWarps * kP * kPitch + (size_t)kFusedWarps * kMaxOv2 * kP) * sizeof(float2);
+}
+
 // patches (of the n per side) covering tile positions [lo, hi]
 void patch_span(const GoldsteinGeom& g, int lo, int hi, int& first, int& count) {
   // patch q covers [q s - ov, q s - ov + p)
@@ -342,6 +543,20 @@ std::vector<GoldsteinTile> goldstein_tiles(const GoldsteinGeom& g) {
   return tiles;
 }
 
+// Patch rows / columns of the fused kernel's bands and strips.
+GoldsteinBands goldstein_bands(const GoldsteinGeom& g) {
+  GoldsteinBands B;
+  // tile rows [ov, H + ov - 2] lie in patch rows 0 .. (H + 2 ov - 2) / s;
+  // tile row sub - ov - 1 (output row H - 1) in patch row n - 1
+  B.rows_main = g.H >= 2 ? (g.H + 2 * g.ov - 2) / g.s + 1 : 0;
+  B.row_far = (g.n - 1 >= B.rows_main) ? g.n - 1 : -1;
+  B.bands_main = (B.rows_main + kBandRows - 1) / kBandRows;
+  B.cols_main = g.W >= 2 ? (g.W + 2 * g.ov - 2) / g.s + 1 : 0;
+  B.col_far = (g.n - 1 >= B.cols_main) ? g.n - 1 : -1;
+  B.strips_main = (B.cols_main + kStripX - 1) / kStripX;
+  return B;
+}
+
 int goldstein_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase, int H, int W, int p,
                      int ov, float alpha, cudaStream_t st) {
   if (!a1 || !a2 || !phi || !ref || !phase) return set_error(DCL_ERR_INVALID_ARGUMENT, "null pointer");
@@ -351,6 +566,19 @@ int goldstein_device(const float* a1, const float* a2, const float* phi, float* 
   int dev = 0;
   rc = ensure_device_ready(dev);
   if (rc) return rc;
+  if (!g_goldstein_two_pass) {
+    const GoldsteinBands B = goldstein_bands(g);
+    const size_t smem = goldstein_fused_smem();
+    static size_t allowed[kMaxDevices];
+    cudaError_t e = allow_dynamic_smem((const void*)goldstein_fused_kernel, smem, allowed);
+    if (e != cudaSuccess) return cuda_error(e, "Goldstein shared memory");
+    const dim3 grid(B.strips_main + (B.col_far >= 0 ? 1 : 0), B.bands_main + (B.row_far >= 0 ? 1 : 0));
+    goldstein_fused_kernel<<<grid, 32 * kFusedWarps, smem, st>>>(a1, a2, phi, ref, phase, g, B, alpha);
+    profile_count(1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "Goldstein launch");
+    return DCL_OK;
+  }
   const std::vector<GoldsteinTile> tiles = goldstein_tiles(g);
   size_t np = 0;
   for (const GoldsteinTile& t : tiles) np = std::max(np, (size_t)t.n_py * t.n_px);
