@@ -13,7 +13,14 @@
 // The result at (y, x) is therefore tile row y / (sub - 2 ov) at tile row
 // y - origin for y < H-1, and the last tile row at tile row sub - ov - 1 for
 // y = H-1 (columns alike).  Per tile, only the patches behind those final
-// positions are filtered.  Two kernels per tile:
+// positions are filtered.  One launch per tile (one tile for most scenes):
+//
+//  goldstein_fused_kernel  patches filtered into shared memory and the
+//     overlap-add of the rows they complete, strip by strip and band by band
+//     (described above the kernel).
+//
+// DESPECKCL_B200_GOLDSTEIN_TWO_PASS=1 selects the same arithmetic in two
+// kernels per tile, patches through HBM:
 //
 //  goldstein_patch_kernel  one warp per patch: gathers the 32 x 32 patch of the
 //     clamp-extended raw interferogram Z = 0.5 (a1 + a2) e^{j phi}
@@ -72,7 +79,9 @@ __host__ __device__ constexpr int rev5(int i) {
 }
 
 // In-register 32-point radix-2 decimation-in-time FFT (forward: e^{-i}, no
-// scaling; inverse: e^{+i}, no scaling).
+// scaling; inverse: e^{+i}, no scaling).  Every product and sum below is an
+// explicitly rounded intrinsic, so the two Goldstein paths of this file, which
+// share these functions, give the same bits whatever the compiler contracts.
 template <bool INV>
 __device__ __forceinline__ void fft32(float2 (&x)[kP]) {
 #pragma unroll
@@ -101,10 +110,10 @@ __device__ __forceinline__ void fft32(float2 (&x)[kP]) {
         } else {
           const float2 w = c_tw32[m];
           const float wy = INV ? -w.y : w.y;
-          t = make_float2(b.x * w.x - b.y * wy, b.x * wy + b.y * w.x);
+          t = make_float2(__fmaf_rn(b.x, w.x, -__fmul_rn(b.y, wy)), __fmaf_rn(b.x, wy, __fmul_rn(b.y, w.x)));
         }
-        x[i + k] = make_float2(a.x + t.x, a.y + t.y);
-        x[i + k + half] = make_float2(a.x - t.x, a.y - t.y);
+        x[i + k] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
+        x[i + k + half] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
       }
     }
   }
@@ -140,28 +149,31 @@ struct GoldsteinTile {
   int x_lo, x_hi;      // output columns likewise
 };
 
-__global__ void __launch_bounds__(32 * kWarps)
-    goldstein_patch_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
-                           float2* __restrict__ patches, GoldsteinGeom g, GoldsteinTile t, float alpha) {
-  __shared__ float2 sbuf[kWarps][kP * kPitch];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int pid = blockIdx.x * kWarps + warp;
-  if (pid >= t.n_py * t.n_px) return;  // whole warp leaves together
-  float2* buf = sbuf[warp];
-  const int py = t.py_lo + pid / t.n_px, px = t.px_lo + pid % t.n_px;
-  // gather: lane = column of the patch
+// Z = 0.5 (a1 + a2) e^{j phi} at flat index i (raw_interferogram.cl)
+__device__ __forceinline__ float2 raw_z(const float* __restrict__ a1, const float* __restrict__ a2,
+                                        const float* __restrict__ phi, size_t i) {
+  const float amp = __fmul_rn(0.5f, __fadd_rn(a1[i], a2[i]));
+  float sn, cs;
+  __sincosf(phi[i], &sn, &cs);
+  return make_float2(__fmul_rn(amp, cs), __fmul_rn(amp, sn));
+}
+
+// Filters patch (py, px) of the tile whose position (0, 0) is image pixel
+// (o0y, o0x) into buf[r * kPitch + c] (row r, column c), one warp: gathers the
+// patch of the clamp-extended raw interferogram (lane = column), 2-D FFT (rows
+// then columns), |Z|^alpha weight, inverse 2-D FFT with the 1/p^2 scale.  The
+// caller synchronises the warp before other lanes read buf.
+__device__ __forceinline__ void filter_patch(const float* __restrict__ a1, const float* __restrict__ a2,
+                                             const float* __restrict__ phi, float2* buf, const GoldsteinGeom& g,
+                                             int o0y, int o0x, int py, int px, float alpha, int lane) {
   {
     const int tx = clampg(px * g.s + lane - g.ov, 0, g.sub - 1);
-    const int ix = clampg(t.w0 + tx, 0, g.W - 1);
+    const int ix = clampg(o0x + tx, 0, g.W - 1);
 #pragma unroll 4
     for (int r = 0; r < kP; ++r) {
       const int ty = clampg(py * g.s + r - g.ov, 0, g.sub - 1);
-      const int iy = clampg(t.h0 + ty, 0, g.H - 1);
-      const size_t i = (size_t)iy * g.W + ix;
-      const float amp = 0.5f * (a1[i] + a2[i]);
-      float sn, cs;
-      __sincosf(phi[i], &sn, &cs);
-      buf[r * kPitch + lane] = make_float2(amp * cs, amp * sn);
+      const int iy = clampg(o0y + ty, 0, g.H - 1);
+      buf[r * kPitch + lane] = raw_z(a1, a2, phi, (size_t)iy * g.W + ix);
     }
   }
   __syncwarp();
@@ -181,9 +193,9 @@ __global__ void __launch_bounds__(32 * kWarps)
   const float half_alpha = 0.5f * alpha;
 #pragma unroll
   for (int r = 0; r < kP; ++r) {
-    const float m2 = x[r].x * x[r].x + x[r].y * x[r].y;
-    const float w = (alpha == 0.0f) ? 1.0f : ex2_approx(half_alpha * __log2f(m2));
-    x[r] = make_float2(w * x[r].x, w * x[r].y);
+    const float m2 = __fmaf_rn(x[r].x, x[r].x, __fmul_rn(x[r].y, x[r].y));
+    const float w = (alpha == 0.0f) ? 1.0f : ex2_approx(__fmul_rn(half_alpha, __log2f(m2)));
+    x[r] = make_float2(__fmul_rn(w, x[r].x), __fmul_rn(w, x[r].y));
   }
   fft32<true>(x);
 #pragma unroll
@@ -195,7 +207,18 @@ __global__ void __launch_bounds__(32 * kWarps)
   fft32<true>(x);
   constexpr float kScale = 1.0f / (kP * kP);
 #pragma unroll
-  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = make_float2(x[k].x * kScale, x[k].y * kScale);
+  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = make_float2(__fmul_rn(x[k].x, kScale), __fmul_rn(x[k].y, kScale));
+}
+
+__global__ void __launch_bounds__(32 * kWarps)
+    goldstein_patch_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
+                           float2* __restrict__ patches, GoldsteinGeom g, GoldsteinTile t, float alpha) {
+  __shared__ float2 sbuf[kWarps][kP * kPitch];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pid = blockIdx.x * kWarps + warp;
+  if (pid >= t.n_py * t.n_px) return;  // whole warp leaves together
+  float2* buf = sbuf[warp];
+  filter_patch(a1, a2, phi, buf, g, t.h0, t.w0, t.py_lo + pid / t.n_px, t.px_lo + pid % t.n_px, alpha, lane);
   __syncwarp();
   float2* out = patches + (size_t)pid * kP * kP;
 #pragma unroll 4
@@ -208,6 +231,19 @@ __device__ __forceinline__ float pack_factor(int rel, int o, int ov, int sub) {
   if (rel < 2 * ov || rel >= kP - 2 * ov) f *= 0.5f;
   if (o < ov || o >= sub - ov) f *= 2.0f;
   return f;
+}
+
+// v += fx fy q (fx fy is a power of two: exact)
+__device__ __forceinline__ void add_sample(float2& v, float fx, float fy, float2 q) {
+  const float f = __fmul_rn(fx, fy);
+  v.x = __fmaf_rn(f, q.x, v.x);
+  v.y = __fmaf_rn(f, q.y, v.y);
+}
+
+// |Z| and arg Z (slc2real.cl)
+__device__ __forceinline__ void write_polar(float* __restrict__ ref, float* __restrict__ phase, size_t o, float2 v) {
+  ref[o] = fabsf(sqrtf(__fmaf_rn(v.x, v.x, __fmul_rn(v.y, v.y))));
+  phase[o] = atan2f(v.y, v.x);
 }
 
 constexpr int kPackX = 4;  // output columns per thread (32 apart: coalesced per warp)
@@ -246,14 +282,7 @@ __global__ void __launch_bounds__(256)
     const int x = x0 + 32 * m;
     if (x > t.x_hi) break;
     const int tx = (x == g.W - 1) ? g.sub - g.ov - 1 : x - t.w0;
-    float2 v;
-    {
-      const size_t i = irow + clampg(t.w0 + tx, 0, g.W - 1);
-      const float amp = 0.5f * (a1[i] + a2[i]);
-      float sn, cs;
-      __sincosf(phi[i], &sn, &cs);
-      v = make_float2(amp * cs, amp * sn);
-    }
+    float2 v = raw_z(a1, a2, phi, irow + clampg(t.w0 + tx, 0, g.W - 1));
     const int qx = div_s(tx + g.ov, g), cx = tx + g.ov - qx * g.s;
     const bool vx0 = qx >= t.px_lo && qx < t.px_lo + t.n_px;
     const bool vx1 = qx - 1 >= t.px_lo && qx - 1 < t.px_lo + t.n_px && cx + g.s < kP;
@@ -275,209 +304,150 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int ypar = 0; ypar < 2; ++ypar) {
         if (!vx_[xpar] || !vy_[ypar]) continue;
-        const float f = fx_[xpar] * fy_[ypar];
-        const float2 q = patches[((size_t)(py_[ypar] - t.py_lo) * t.n_px + (px_[xpar] - t.px_lo)) * kP * kP +
-                                 ry_[ypar] * kP + cx_[xpar]];
-        v.x += f * q.x;
-        v.y += f * q.y;
+        add_sample(v, fx_[xpar], fy_[ypar],
+                   patches[((size_t)(py_[ypar] - t.py_lo) * t.n_px + (px_[xpar] - t.px_lo)) * kP * kP +
+                           ry_[ypar] * kP + cx_[xpar]]);
       }
-    const size_t o = (size_t)y * g.W + x;
-    ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
-    phase[o] = atan2f(v.y, v.x);
+    write_polar(ref, phase, (size_t)y * g.W + x, v);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Fused kernel: patch FFTs and the overlap-add in one launch, no patch scratch
-// in HBM.  A CTA owns a strip of kStripX patch columns and a band of patch
-// rows of the (single) tile.  Its kStripX + 1 warps filter one patch each per
-// patch row (the extra warp the column left of the strip, whose right edge
-// overlaps it), then every thread adds, for the tile rows whose covering
-// patches are all filtered now, the raw interferogram and the weighted patch
-// samples in the reference's parity order and writes |Z| and arg Z.  A tile row
-// is covered by its patch row q and, in its first 2 ov rows, by q - 1: the last
-// 2 ov rows of every filtered patch are kept in shared memory for the next
-// patch row, so each patch is filtered once per strip and band (plus one row
-// and one column of overlap with the neighbouring CTAs).
+// Fused kernel: patch FFTs and the overlap-add in one launch per tile, no
+// patch scratch in HBM.  A CTA owns a strip of kStripX patch columns and a
+// band of patch rows of one tile.  Its kStripX + 1 warps filter one patch each
+// per patch row (the extra warp the column left of the strip, whose right
+// edge overlaps it) into shared memory; then every warp takes tile rows, every
+// lane tile columns, of the rows whose covering patches are all filtered now,
+// adds the raw interferogram and the weighted patch samples in the
+// reference's parity order and writes |Z| and arg Z.  A tile row is covered by
+// its patch row q and, in its first 2 ov rows, by q - 1: the last 2 ov rows of
+// every filtered patch stay in shared memory for the next patch row, so each
+// patch is filtered once per strip and band (plus one row and one column of
+// overlap with the neighbouring CTAs).  Per tile column, the output column,
+// the image column, the covering patches' buffer offsets and weights are
+// tabulated once per CTA in shared memory.
 // ---------------------------------------------------------------------------
 
 constexpr int kStripX = 7;              // patch columns finalised per CTA
 constexpr int kFusedWarps = kStripX + 1;
 constexpr int kBandRows = 16;           // patch rows finalised per CTA
 constexpr int kMaxOv2 = kP / 2 - 1;     // 2 ov < p / 2
+constexpr int kMaxNx = kStripX * kP;    // tile columns finalised per CTA, at most
 
-struct GoldsteinBands {
-  int rows_main;   // patch rows 0 .. rows_main - 1 hold tile rows [ov, H + ov - 2]
-  int row_far;     // patch row of tile row sub - ov - 1 when it lies past them, else -1
-  int bands_main;  // ceil(rows_main / kBandRows)
-  int cols_main, col_far, strips_main;  // the same for columns (kStripX per strip)
+// One axis (rows or columns) of a tile, for the fused kernel.
+struct GoldsteinAxis {
+  int o0;      // image index of tile position 0
+  int lo, hi;  // outputs o <= N - 2 taken at tile position o - o0 (none when lo > hi)
+  int last;    // output N - 1 taken at tile position sub - ov - 1
+  int q_lo;    // first patch holding positions [lo - o0, hi - o0]
+  int n_main;  // patches q_lo .. q_lo + n_main - 1
+  int q_far;   // patch n - 1 (position sub - ov - 1) when it lies past them, else -1
+  int groups;  // CTAs along the axis
 };
 
-__device__ __forceinline__ void filter_patch(const float* __restrict__ a1, const float* __restrict__ a2,
-                                             const float* __restrict__ phi, float2* buf, const GoldsteinGeom& g,
-                                             int py, int px, float alpha, int lane) {
-  // gather: lane = column of the patch (the clamp-extended raw interferogram)
-  {
-    const int tx = clampg(px * g.s + lane - g.ov, 0, g.sub - 1);
-    const int ix = clampg(tx - g.ov, 0, g.W - 1);
-#pragma unroll 4
-    for (int r = 0; r < kP; ++r) {
-      const int ty = clampg(py * g.s + r - g.ov, 0, g.sub - 1);
-      const int iy = clampg(ty - g.ov, 0, g.H - 1);
-      const size_t i = (size_t)iy * g.W + ix;
-      const float amp = 0.5f * (a1[i] + a2[i]);
-      float sn, cs;
-      __sincosf(phi[i], &sn, &cs);
-      buf[r * kPitch + lane] = make_float2(amp * cs, amp * sn);
-    }
-  }
-  __syncwarp();
-  float2 x[kP];
-#pragma unroll
-  for (int k = 0; k < kP; ++k) x[k] = buf[lane * kPitch + k];
-  fft32<false>(x);
-#pragma unroll
-  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = x[k];
-  __syncwarp();
-#pragma unroll
-  for (int r = 0; r < kP; ++r) x[r] = buf[r * kPitch + lane];
-  fft32<false>(x);
-  const float half_alpha = 0.5f * alpha;
-#pragma unroll
-  for (int r = 0; r < kP; ++r) {
-    const float m2 = x[r].x * x[r].x + x[r].y * x[r].y;
-    const float w = (alpha == 0.0f) ? 1.0f : ex2_approx(half_alpha * __log2f(m2));
-    x[r] = make_float2(w * x[r].x, w * x[r].y);
-  }
-  fft32<true>(x);
-#pragma unroll
-  for (int r = 0; r < kP; ++r) buf[r * kPitch + lane] = x[r];
-  __syncwarp();
-#pragma unroll
-  for (int k = 0; k < kP; ++k) x[k] = buf[lane * kPitch + k];
-  fft32<true>(x);
-  constexpr float kScale = 1.0f / (kP * kP);
-#pragma unroll
-  for (int k = 0; k < kP; ++k) buf[lane * kPitch + k] = make_float2(x[k].x * kScale, x[k].y * kScale);
+// output index of tile position t, or -1 when no output takes its value
+__device__ __forceinline__ int axis_out(const GoldsteinAxis& a, int t, int n_out, const GoldsteinGeom& g) {
+  if (a.last && t == g.sub - g.ov - 1) return n_out - 1;
+  const int o = t + a.o0;
+  return (o >= a.lo && o <= a.hi) ? o : -1;
 }
 
-// tile position t -> output index (row or column), or -1 when no output
-// takes its value: t = o + ov for o < N - 1, t = sub - ov - 1 for o = N - 1
-__device__ __forceinline__ int out_of_tile(int t, int n_out, const GoldsteinGeom& g) {
-  if (t == g.sub - g.ov - 1) return n_out - 1;
-  const int o = t - g.ov;
-  return (o >= 0 && o < n_out - 1) ? o : -1;
+// patches [r0, r1) of CTA b along an axis cut into groups of G
+__device__ __forceinline__ void axis_range(const GoldsteinAxis& a, int b, int G, int& r0, int& r1) {
+  const int main_groups = (a.n_main + G - 1) / G;
+  if (b < main_groups) {
+    r0 = a.q_lo + b * G;
+    r1 = min(r0 + G, a.q_lo + a.n_main);
+  } else {
+    r0 = a.q_far;
+    r1 = r0 + 1;
+  }
 }
 
 __global__ void __launch_bounds__(32 * kFusedWarps, 2)
     goldstein_fused_kernel(const float* __restrict__ a1, const float* __restrict__ a2,
                            const float* __restrict__ phi, float* __restrict__ ref, float* __restrict__ phase,
-                           GoldsteinGeom g, GoldsteinBands B, float alpha) {
+                           GoldsteinGeom g, GoldsteinAxis ay, GoldsteinAxis ax, float alpha) {
   extern __shared__ float2 gsm[];
-  float2* cur = gsm;                                       // [warps][kP * kPitch]
-  float2* prev = gsm + (size_t)kFusedWarps * kP * kPitch;  // [warps][2 ov][kP]
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ov2 = 2 * g.ov;
-  // this CTA's patch columns (finalised: [c0, c1)) and patch rows ([r0, r1))
+  float2* cur = gsm;                                 // [warps][kP][kPitch]: this patch row
+  float2* prev = cur + kFusedWarps * kP * kPitch;    // [warps][2 ov][kP]: the last 2 ov rows of the previous one
+  int* t_xo = reinterpret_cast<int*>(prev + kFusedWarps * ov2 * kP);  // output column (-1: none)
+  int* t_icol = t_xo + kMaxNx;                       // image column of the raw interferogram
+  int* t_cb = t_icol + kMaxNx;                       // [2]: offset in cur of the even / odd column's patch
+  int* t_pb = t_cb + 2 * kMaxNx;                     // [2]: the same in prev
+  float* t_fx = reinterpret_cast<float*>(t_pb + 2 * kMaxNx);  // [2]: column weight (0: not covering)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int c0, c1, r0, r1;
-  if ((int)blockIdx.x < B.strips_main) {
-    c0 = blockIdx.x * kStripX;
-    c1 = min(c0 + kStripX, B.cols_main);
-  } else {
-    c0 = B.col_far;
-    c1 = c0 + 1;
-  }
-  if ((int)blockIdx.y < B.bands_main) {
-    r0 = blockIdx.y * kBandRows;
-    r1 = min(r0 + kBandRows, B.rows_main);
-  } else {
-    r0 = B.row_far;
-    r1 = r0 + 1;
+  axis_range(ax, blockIdx.x, kStripX, c0, c1);
+  axis_range(ay, blockIdx.y, kBandRows, r0, r1);
+  const int nx = (c1 - c0) * g.s;
+  const int tx_lo = c0 * g.s - g.ov;
+  for (int cxr = threadIdx.x; cxr < nx; cxr += blockDim.x) {
+    // tile column tx: patch column qx = c0 + k at offset cx, and qx - 1 at
+    // cx + s for cx < 2 ov; the warp of patch column c0 - 1 + w is w
+    const int tx = tx_lo + cxr;
+    const int k = div_s(cxr, g);
+    const int qx = c0 + k, cx = cxr - k * g.s;
+    t_xo[cxr] = axis_out(ax, tx, g.W, g);
+    t_icol[cxr] = clampg(ax.o0 + tx, 0, g.W - 1);
+    const int own = qx & 1, oth = own ^ 1;
+    t_cb[own * kMaxNx + cxr] = (k + 1) * kP * kPitch + cx;
+    t_pb[own * kMaxNx + cxr] = (k + 1) * ov2 * kP + cx;
+    t_fx[own * kMaxNx + cxr] = pack_factor(cx, tx, g.ov, g.sub);
+    const bool v1 = qx >= 1 && cx < ov2;
+    t_cb[oth * kMaxNx + cxr] = v1 ? k * kP * kPitch + cx + g.s : 0;
+    t_pb[oth * kMaxNx + cxr] = v1 ? k * ov2 * kP + cx + g.s : 0;
+    t_fx[oth * kMaxNx + cxr] = v1 ? pack_factor(cx + g.s, tx, g.ov, g.sub) : 0.0f;
   }
   const int pxw = c0 - 1 + warp;  // this warp's patch column
   const bool col_ok = pxw >= 0 && pxw < c1;
-  float2* mycur = cur + (size_t)warp * kP * kPitch;
-  float2* myprev = prev + (size_t)warp * kMaxOv2 * kP;
-  const int tx_lo = c0 * g.s - g.ov, tx_hi = c1 * g.s - g.ov;  // tile columns finalised
-  const int nx = tx_hi - tx_lo;
-  const float inv_nx = 1.0f / (float)nx;
+  float2* mycur = cur + warp * kP * kPitch;
+  float2* myprev = prev + warp * ov2 * kP;
   for (int q = max(r0 - 1, 0); q < r1; ++q) {
-    if (col_ok) filter_patch(a1, a2, phi, mycur, g, q, pxw, alpha, lane);
-    __syncthreads();
+    if (col_ok) filter_patch(a1, a2, phi, mycur, g, ay.o0, ax.o0, q, pxw, alpha, lane);
+    __syncthreads();  // patches of row q (and, the first time, the column tables) visible
     if (q >= r0) {
-      // tile rows [q s - ov, (q + 1) s - ov): patch row q at offset ry, and
-      // q - 1 at ry + s for ry < 2 ov
-      const int ty_lo = q * g.s - g.ov;
-      for (int it = threadIdx.x; it < g.s * nx; it += blockDim.x) {
-        // it / nx and cxr / s by a float estimate corrected to the exact
-        // quotient (it < 2^24)
-        int ry = __float2int_rz((float)it * inv_nx);
-        if (ry * nx > it) --ry;
-        if ((ry + 1) * nx <= it) ++ry;
-        const int cxr = it - ry * nx;
-        const int ty = ty_lo + ry, tx = tx_lo + cxr;
-        const int y = out_of_tile(ty, g.H, g), x = out_of_tile(tx, g.W, g);
-        if (y < 0 || x < 0) continue;
-        const size_t i = (size_t)clampg(ty - g.ov, 0, g.H - 1) * g.W + clampg(tx - g.ov, 0, g.W - 1);
-        float2 v;
-        {
-          const float amp = 0.5f * (a1[i] + a2[i]);
-          float sn, cs;
-          __sincosf(phi[i], &sn, &cs);
-          v = make_float2(amp * cs, amp * sn);
-        }
-        // covering patches: row q (offset ry) and q - 1 (offset ry + s);
-        // column qx = (tx + ov) / s (offset cx) and qx - 1 (offset cx + s)
-        const int qx = c0 + div_s(cxr, g), cx = cxr - (qx - c0) * g.s;
-        const bool vy1 = q >= 1 && ry < ov2;
-        const bool vx1 = qx >= 1 && cx < ov2;
-        const bool ye1 = q & 1, xe1 = qx & 1;
-        // index 0: the even patch, 1: the odd one (the reference's parity launches)
-        float fy[2], fx[2];
-        bool vy[2], vx[2];
-        vy[ye1 ? 1 : 0] = true;
-        vy[ye1 ? 0 : 1] = vy1;
-        vx[xe1 ? 1 : 0] = true;
-        vx[xe1 ? 0 : 1] = vx1;
-        fy[ye1 ? 1 : 0] = pack_factor(ry, ty, g.ov, g.sub);
-        fy[ye1 ? 0 : 1] = pack_factor(ry + g.s, ty, g.ov, g.sub);
-        fx[xe1 ? 1 : 0] = pack_factor(cx, tx, g.ov, g.sub);
-        fx[xe1 ? 0 : 1] = pack_factor(cx + g.s, tx, g.ov, g.sub);
-        // warp of patch column qx is qx - c0 + 1; of qx - 1, qx - c0
-        const int wq = qx - c0 + 1;
+      // tile rows [q s - ov, (q + 1) s - ov): patch row q at offset ry (cur)
+      // and q - 1 at ry + s for ry < 2 ov (prev); slot 0 is the even one
+      const bool odd = q & 1;
+      for (int ry = warp; ry < g.s; ry += kFusedWarps) {
+        const int ty = q * g.s - g.ov + ry;
+        const int y = axis_out(ay, ty, g.H, g);
+        if (y < 0) continue;
+        const size_t irow = (size_t)clampg(ay.o0 + ty, 0, g.H - 1) * g.W;
+        const float f_own = pack_factor(ry, ty, g.ov, g.sub);
+        const float f_oth = (q >= 1 && ry < ov2) ? pack_factor(ry + g.s, ty, g.ov, g.sub) : 0.0f;
+        const float fy0 = odd ? f_oth : f_own, fy1 = odd ? f_own : f_oth;
+        const int rc = ry * kPitch, rp = ry * kP;
+        for (int cxr = lane; cxr < nx; cxr += 32) {
+          const int x = t_xo[cxr];
+          if (x < 0) continue;
+          float2 v = raw_z(a1, a2, phi, irow + t_icol[cxr]);
 #pragma unroll
-        for (int xpar = 0; xpar < 2; ++xpar)
-#pragma unroll
-          for (int ypar = 0; ypar < 2; ++ypar) {
-            if (!vx[xpar] || !vy[ypar]) continue;
-            const bool xcur = (xpar == 1) == xe1;  // the column qx itself
-            const bool ycur = (ypar == 1) == ye1;  // the row q itself
-            const int w = xcur ? wq : wq - 1;
-            const int c = xcur ? cx : cx + g.s;
-            const float2 smp = ycur ? cur[(size_t)w * kP * kPitch + ry * kPitch + c]
-                                    : prev[(size_t)w * kMaxOv2 * kP + ry * kP + c];
-            const float f = fx[xpar] * fy[ypar];
-            v.x += f * smp.x;
-            v.y += f * smp.y;
+          for (int xpar = 0; xpar < 2; ++xpar) {
+            const float fx = t_fx[xpar * kMaxNx + cxr];
+            if (fx == 0.0f) continue;
+            const int cb = t_cb[xpar * kMaxNx + cxr] + rc, pb = t_pb[xpar * kMaxNx + cxr] + rp;
+            if (fy0 != 0.0f) add_sample(v, fx, fy0, odd ? prev[pb] : cur[cb]);
+            if (fy1 != 0.0f) add_sample(v, fx, fy1, odd ? cur[cb] : prev[pb]);
           }
-        const size_t o = (size_t)y * g.W + x;
-        ref[o] = fabsf(sqrtf(v.x * v.x + v.y * v.y));
-        phase[o] = atan2f(v.y, v.x);
+          write_polar(ref, phase, (size_t)y * g.W + x, v);
+        }
       }
     }
-    __syncthreads();
+    __syncthreads();  // every read of cur and prev done
     // keep the last 2 ov rows of this patch row for the next one
     if (col_ok)
-      for (int k = lane; k < ov2 * kP; k += 32) {
-        const int r = k / kP, c = k - r * kP;
-        myprev[k] = mycur[(g.s + r) * kPitch + c];
-      }
+      for (int k = lane; k < ov2 * kP; k += 32) myprev[k] = mycur[(g.s + (k >> 5)) * kPitch + (k & 31)];
     __syncwarp();
   }
 }
 
-size_t goldstein_fused_smem() {
-  return ((size_t)kFusedWarps * kP * kPitch + (size_t)kFusedWarps * kMaxOv2 * kP) * sizeof(float2);
+size_t goldstein_fused_smem(int ov) {
+  return ((size_t)kFusedWarps * kP * kPitch + (size_t)kFusedWarps * 2 * ov * kP) * sizeof(float2) +
+         (size_t)8 * kMaxNx * sizeof(int);
 }
 
 // patches (of the n per side) covering tile positions [lo, hi]
@@ -513,7 +483,9 @@ int goldstein_geom(int H, int W, int p, int ov, GoldsteinGeom& g) {
 
 // The reference's tiles (tile_iterator.cpp with tile side g.sub and overlap
 // ov) and, per tile, the output rectangle it finally owns and the patches
-// behind it.
+// behind it.  A scene has one tile per axis unless sub - 3 ov < H (W), i.e.
+// (max(H, W) + 2 ov) mod s > s - ov: then a second tile holds the last
+// outputs, read from its own clamp-extended neighbourhood.
 std::vector<GoldsteinTile> goldstein_tiles(const GoldsteinGeom& g) {
   const int step = g.sub - 2 * g.ov;
   std::vector<int> h0s, w0s;
@@ -543,18 +515,27 @@ std::vector<GoldsteinTile> goldstein_tiles(const GoldsteinGeom& g) {
   return tiles;
 }
 
-// Patch rows / columns of the fused kernel's bands and strips.
-GoldsteinBands goldstein_bands(const GoldsteinGeom& g) {
-  GoldsteinBands B;
-  // tile rows [ov, H + ov - 2] lie in patch rows 0 .. (H + 2 ov - 2) / s;
-  // tile row sub - ov - 1 (output row H - 1) in patch row n - 1
-  B.rows_main = g.H >= 2 ? (g.H + 2 * g.ov - 2) / g.s + 1 : 0;
-  B.row_far = (g.n - 1 >= B.rows_main) ? g.n - 1 : -1;
-  B.bands_main = (B.rows_main + kBandRows - 1) / kBandRows;
-  B.cols_main = g.W >= 2 ? (g.W + 2 * g.ov - 2) / g.s + 1 : 0;
-  B.col_far = (g.n - 1 >= B.cols_main) ? g.n - 1 : -1;
-  B.strips_main = (B.cols_main + kStripX - 1) / kStripX;
-  return B;
+// One axis of a tile for the fused kernel: outputs [lo, hi_incl] of n_out,
+// patches grouped by `group` per CTA.
+GoldsteinAxis goldstein_axis(const GoldsteinGeom& g, int o0, int lo, int hi_incl, int n_out, int group) {
+  GoldsteinAxis a;
+  a.o0 = o0;
+  a.lo = lo;
+  a.hi = std::min(hi_incl, n_out - 2);
+  a.last = hi_incl == n_out - 1;
+  a.q_lo = 0;
+  a.n_main = 0;
+  int q_hi = -1;
+  if (a.lo <= a.hi) {
+    // tile positions [lo - o0, hi - o0] (>= 0: o0 >= -ov) in patches (t + ov) / s
+    a.q_lo = (a.lo - o0 + g.ov) / g.s;
+    q_hi = (a.hi - o0 + g.ov) / g.s;
+    a.n_main = q_hi - a.q_lo + 1;
+  }
+  const int q_last = g.n - 1;  // (sub - ov - 1 + ov) / s
+  a.q_far = (a.last && !(a.n_main > 0 && q_last >= a.q_lo && q_last <= q_hi)) ? q_last : -1;
+  a.groups = (a.n_main + group - 1) / group + (a.q_far >= 0 ? 1 : 0);
+  return a;
 }
 
 int goldstein_device(const float* a1, const float* a2, const float* phi, float* ref, float* phase, int H, int W, int p,
@@ -566,20 +547,25 @@ int goldstein_device(const float* a1, const float* a2, const float* phi, float* 
   int dev = 0;
   rc = ensure_device_ready(dev);
   if (rc) return rc;
+  const std::vector<GoldsteinTile> tiles = goldstein_tiles(g);
   if (!g_goldstein_two_pass) {
-    const GoldsteinBands B = goldstein_bands(g);
-    const size_t smem = goldstein_fused_smem();
+    const size_t smem = goldstein_fused_smem(ov);
     static size_t allowed[kMaxDevices];
-    cudaError_t e = allow_dynamic_smem((const void*)goldstein_fused_kernel, smem, allowed);
+    cudaError_t e = allow_dynamic_smem((const void*)goldstein_fused_kernel, goldstein_fused_smem(kMaxOv2 / 2), allowed);
     if (e != cudaSuccess) return cuda_error(e, "Goldstein shared memory");
-    const dim3 grid(B.strips_main + (B.col_far >= 0 ? 1 : 0), B.bands_main + (B.row_far >= 0 ? 1 : 0));
-    goldstein_fused_kernel<<<grid, 32 * kFusedWarps, smem, st>>>(a1, a2, phi, ref, phase, g, B, alpha);
-    profile_count(1);
+    // tiles own disjoint outputs: one launch each (one for most scenes)
+    for (const GoldsteinTile& t : tiles) {
+      const GoldsteinAxis ay = goldstein_axis(g, t.h0, t.y_lo, t.y_hi, H, kBandRows);
+      const GoldsteinAxis ax = goldstein_axis(g, t.w0, t.x_lo, t.x_hi, W, kStripX);
+      if (ay.groups == 0 || ax.groups == 0) continue;
+      goldstein_fused_kernel<<<dim3(ax.groups, ay.groups), 32 * kFusedWarps, smem, st>>>(a1, a2, phi, ref, phase, g,
+                                                                                        ay, ax, alpha);
+      profile_count(1);
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "Goldstein launch");
     return DCL_OK;
   }
-  const std::vector<GoldsteinTile> tiles = goldstein_tiles(g);
   size_t np = 0;
   for (const GoldsteinTile& t : tiles) np = std::max(np, (size_t)t.n_py * t.n_px);
   float2* patches = nullptr;
