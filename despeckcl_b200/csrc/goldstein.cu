@@ -13,14 +13,7 @@
 // The result at (y, x) is therefore tile row y / (sub - 2 ov) at tile row
 // y - origin for y < H-1, and the last tile row at tile row sub - ov - 1 for
 // y = H-1 (columns alike).  Per tile, only the patches behind those final
-// positions are filtered.  One launch per tile (one tile for most scenes):
-//
-//  goldstein_fused_kernel  patches filtered into shared memory and the
-//     overlap-add of the rows they complete, strip by strip and band by band
-//     (described above the kernel).
-//
-// DESPECKCL_B200_GOLDSTEIN_TWO_PASS=1 selects the same arithmetic in two
-// kernels per tile, patches through HBM:
+// positions are filtered.  Two kernels per tile:
 //
 //  goldstein_patch_kernel  one warp per patch: gathers the 32 x 32 patch of the
 //     clamp-extended raw interferogram Z = 0.5 (a1 + a2) e^{j phi}
@@ -37,6 +30,16 @@
 //     (patches_pack.cl:29-71, patches_pack.cpp:48-77); then |Z| and arg Z
 //     (slc2real.cl).  Output row H-1 (column W-1) takes the last tile row
 //     (column) of the clamped write-back (sub_images.cpp:47-69).
+//
+// DESPECKCL_B200_GOLDSTEIN_FUSED=1 selects goldstein_fused_kernel instead, the
+// same arithmetic in one warp-specialised launch per tile with the patches
+// kept in shared memory (described above the kernel).  Both give the same
+// bits.  On B200 the two kernels are faster at every measured size (8192^2:
+// 1.09 ms against 1.56 ms): the fused kernel's ring of patch rows (205 KB)
+// leaves one CTA of 16 warps per SM, half of them FFTs and half latency-bound
+// overlap-add, while the patch kernel runs 24 warps per SM and the pack kernel
+// up to 64, and the patches' round trip through HBM (~28 B per output pixel)
+// hides behind their compute.
 // The coherence output is not written, as in the reference.
 
 #include <cuda_runtime.h>
@@ -51,10 +54,10 @@
 namespace dcl {
 namespace {
 
-// DESPECKCL_B200_GOLDSTEIN_TWO_PASS=1: the two-kernel path (patches through
-// HBM), kept to compare the fused kernel against bit for bit
-const bool g_goldstein_two_pass = [] {
-  const char* v = std::getenv("DESPECKCL_B200_GOLDSTEIN_TWO_PASS");
+// DESPECKCL_B200_GOLDSTEIN_FUSED=1: the fused kernel instead of the two
+// kernels per tile (same bits; slower on B200)
+const bool g_goldstein_fused = [] {
+  const char* v = std::getenv("DESPECKCL_B200_GOLDSTEIN_FUSED");
   return v && v[0] == '1';
 }();
 
@@ -314,26 +317,44 @@ __global__ void __launch_bounds__(256)
 
 // ---------------------------------------------------------------------------
 // Fused kernel: patch FFTs and the overlap-add in one launch per tile, no
-// patch scratch in HBM.  A CTA owns a strip of kStripX patch columns and a
-// band of patch rows of one tile.  Its kStripX + 1 warps filter one patch each
-// per patch row (the extra warp the column left of the strip, whose right
-// edge overlaps it) into shared memory; then every warp takes tile rows, every
-// lane tile columns, of the rows whose covering patches are all filtered now,
-// adds the raw interferogram and the weighted patch samples in the
-// reference's parity order and writes |Z| and arg Z.  A tile row is covered by
-// its patch row q and, in its first 2 ov rows, by q - 1: the last 2 ov rows of
-// every filtered patch stay in shared memory for the next patch row, so each
-// patch is filtered once per strip and band (plus one row and one column of
-// overlap with the neighbouring CTAs).  Per tile column, the output column,
-// the image column, the covering patches' buffer offsets and weights are
-// tabulated once per CTA in shared memory.
+// patch scratch in HBM, warp-specialised.  A CTA works on a strip of kStripX
+// patch columns of one tile at a time, patch row by patch row.  Its
+// kStripX + 1 producer warps filter one patch each per patch row (the extra
+// warp the column left of the strip, whose right edge overlaps it) into a
+// ring of three patch-row buffers in shared memory; its consumer warps take
+// the tile rows of patch row q - one warp a row, one lane a column - while
+// the producers filter row q + 1: raw interferogram plus the weighted samples
+// of patch rows q and q - 1 (both still in the ring) in the reference's parity
+// order, then |Z| and arg Z.  Each patch is filtered once per strip and run of
+// rows (plus one row per run and one column per strip of overlap).  Per tile
+// column, the output column, the image column, the covering patches' buffer
+// offsets and weights are tabulated in shared memory once per strip.
+//
+// Hand-offs use named barriers, each bar.arrive by one side matched by a
+// bar.sync of the other (256 + 256 threads): step k of a run filters patch row
+// q_start + k into ring slot k % 3; the consumers finalise it after FULL(k);
+// the producers write slot k % 3 again (step k + 3 ... as step k') only after
+// EMPTY(k' - 2), the consumers' release of step k' - 2, the last reader of that
+// slot as the previous row.  FULL and EMPTY alternate between two hardware
+// barriers by the parity of k, so one side can never arrive twice on a
+// barrier generation the other side has not passed.
 // ---------------------------------------------------------------------------
 
-constexpr int kStripX = 7;              // patch columns finalised per CTA
-constexpr int kFusedWarps = kStripX + 1;
-constexpr int kBandRows = 16;           // patch rows finalised per CTA
-constexpr int kMaxOv2 = kP / 2 - 1;     // 2 ov < p / 2
-constexpr int kMaxNx = kStripX * kP;    // tile columns finalised per CTA, at most
+constexpr int kStripX = 7;                   // patch columns finalised per CTA
+constexpr int kProducers = kStripX + 1;      // producer warps
+constexpr int kConsumers = 8;                // consumer warps
+constexpr int kFusedThreads = 32 * (kProducers + kConsumers);
+constexpr int kRing = 3;                     // patch-row buffers
+constexpr int kSlot = kProducers * kP * kPitch;  // float2 per patch-row buffer
+constexpr int kMaxNx = kStripX * kP;         // tile columns finalised per CTA, at most
+constexpr int kBarFull = 1, kBarEmpty = 3;   // named barriers 1-2 and 3-4 (0 is __syncthreads)
+
+__device__ __forceinline__ void bar_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kFusedThreads) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(int id) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "n"(kFusedThreads) : "memory");
+}
 
 // One axis (rows or columns) of a tile, for the fused kernel.
 struct GoldsteinAxis {
@@ -343,7 +364,7 @@ struct GoldsteinAxis {
   int q_lo;    // first patch holding positions [lo - o0, hi - o0]
   int n_main;  // patches q_lo .. q_lo + n_main - 1
   int q_far;   // patch n - 1 (position sub - ov - 1) when it lies past them, else -1
-  int groups;  // CTAs along the axis
+  int groups;  // groups of `group` patches along the axis (strips of columns)
 };
 
 // output index of tile position t, or -1 when no output takes its value
@@ -353,7 +374,7 @@ __device__ __forceinline__ int axis_out(const GoldsteinAxis& a, int t, int n_out
   return (o >= a.lo && o <= a.hi) ? o : -1;
 }
 
-// patches [r0, r1) of CTA b along an axis cut into groups of G
+// patches [r0, r1) of group b along an axis cut into groups of G
 __device__ __forceinline__ void axis_range(const GoldsteinAxis& a, int b, int G, int& r0, int& r1) {
   const int main_groups = (a.n_main + G - 1) / G;
   if (b < main_groups) {
@@ -365,54 +386,72 @@ __device__ __forceinline__ void axis_range(const GoldsteinAxis& a, int b, int G,
   }
 }
 
-__global__ void __launch_bounds__(32 * kFusedWarps, 2)
-    goldstein_fused_kernel(const float* __restrict__ a1, const float* __restrict__ a2,
-                           const float* __restrict__ phi, float* __restrict__ ref, float* __restrict__ phase,
-                           GoldsteinGeom g, GoldsteinAxis ay, GoldsteinAxis ax, float alpha) {
-  extern __shared__ float2 gsm[];
-  const int ov2 = 2 * g.ov;
-  float2* cur = gsm;                                 // [warps][kP][kPitch]: this patch row
-  float2* prev = cur + kFusedWarps * kP * kPitch;    // [warps][2 ov][kP]: the last 2 ov rows of the previous one
-  int* t_xo = reinterpret_cast<int*>(prev + kFusedWarps * ov2 * kP);  // output column (-1: none)
-  int* t_icol = t_xo + kMaxNx;                       // image column of the raw interferogram
-  int* t_cb = t_icol + kMaxNx;                       // [2]: offset in cur of the even / odd column's patch
-  int* t_pb = t_cb + 2 * kMaxNx;                     // [2]: the same in prev
-  float* t_fx = reinterpret_cast<float*>(t_pb + 2 * kMaxNx);  // [2]: column weight (0: not covering)
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int c0, c1, r0, r1;
-  axis_range(ax, blockIdx.x, kStripX, c0, c1);
-  axis_range(ay, blockIdx.y, kBandRows, r0, r1);
-  const int nx = (c1 - c0) * g.s;
-  const int tx_lo = c0 * g.s - g.ov;
+// Shared-memory layout of the fused kernel.
+struct FusedSmem {
+  float2* ring;  // [kRing][producer warp][kP][kPitch]: filtered patch rows
+  int* t_xo;     // per tile column of the strip: output column (-1: none)
+  int* t_icol;   // image column of the raw interferogram
+  int* t_cb;     // [2]: offset in a ring slot of the even / odd covering patch column's sample
+  float* t_fx;   // [2]: column weight (0: the patch does not cover the column)
+};
+
+// Column tables of the strip of patch columns [c0, c1).
+__device__ __forceinline__ void fused_tables(const FusedSmem& S, const GoldsteinGeom& g, const GoldsteinAxis& ax,
+                                             int c0, int c1) {
+  const int ov2 = 2 * g.ov, nx = (c1 - c0) * g.s, tx_lo = c0 * g.s - g.ov;
   for (int cxr = threadIdx.x; cxr < nx; cxr += blockDim.x) {
     // tile column tx: patch column qx = c0 + k at offset cx, and qx - 1 at
-    // cx + s for cx < 2 ov; the warp of patch column c0 - 1 + w is w
+    // cx + s for cx < 2 ov; the producer warp of patch column c0 - 1 + w is w
     const int tx = tx_lo + cxr;
     const int k = div_s(cxr, g);
     const int qx = c0 + k, cx = cxr - k * g.s;
-    t_xo[cxr] = axis_out(ax, tx, g.W, g);
-    t_icol[cxr] = clampg(ax.o0 + tx, 0, g.W - 1);
+    S.t_xo[cxr] = axis_out(ax, tx, g.W, g);
+    S.t_icol[cxr] = clampg(ax.o0 + tx, 0, g.W - 1);
     const int own = qx & 1, oth = own ^ 1;
-    t_cb[own * kMaxNx + cxr] = (k + 1) * kP * kPitch + cx;
-    t_pb[own * kMaxNx + cxr] = (k + 1) * ov2 * kP + cx;
-    t_fx[own * kMaxNx + cxr] = pack_factor(cx, tx, g.ov, g.sub);
+    S.t_cb[own * kMaxNx + cxr] = (k + 1) * kP * kPitch + cx;
+    S.t_fx[own * kMaxNx + cxr] = pack_factor(cx, tx, g.ov, g.sub);
     const bool v1 = qx >= 1 && cx < ov2;
-    t_cb[oth * kMaxNx + cxr] = v1 ? k * kP * kPitch + cx + g.s : 0;
-    t_pb[oth * kMaxNx + cxr] = v1 ? k * ov2 * kP + cx + g.s : 0;
-    t_fx[oth * kMaxNx + cxr] = v1 ? pack_factor(cx + g.s, tx, g.ov, g.sub) : 0.0f;
+    S.t_cb[oth * kMaxNx + cxr] = v1 ? k * kP * kPitch + cx + g.s : 0;
+    S.t_fx[oth * kMaxNx + cxr] = v1 ? pack_factor(cx + g.s, tx, g.ov, g.sub) : 0.0f;
   }
-  const int pxw = c0 - 1 + warp;  // this warp's patch column
-  const bool col_ok = pxw >= 0 && pxw < c1;
-  float2* mycur = cur + warp * kP * kPitch;
-  float2* myprev = prev + warp * ov2 * kP;
-  for (int q = max(r0 - 1, 0); q < r1; ++q) {
-    if (col_ok) filter_patch(a1, a2, phi, mycur, g, ay.o0, ax.o0, q, pxw, alpha, lane);
-    __syncthreads();  // patches of row q (and, the first time, the column tables) visible
-    if (q >= r0) {
-      // tile rows [q s - ov, (q + 1) s - ov): patch row q at offset ry (cur)
-      // and q - 1 at ry + s for ry < 2 ov (prev); slot 0 is the even one
+}
+
+// One run: patch rows [qa, qb) of the strip [c0, c1) finalised, patch row
+// qa - 1 filtered first (for the first 2 ov tile rows of qa).  Block-uniform
+// arguments; every thread of the block calls it.
+__device__ __forceinline__ void fused_run(const float* __restrict__ a1, const float* __restrict__ a2,
+                                          const float* __restrict__ phi, float* __restrict__ ref,
+                                          float* __restrict__ phase, const FusedSmem& S, const GoldsteinGeom& g,
+                                          const GoldsteinAxis& ay, const GoldsteinAxis& ax, float alpha, int c0,
+                                          int c1, int qa, int qb) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q_start = max(qa - 1, 0);
+  const int K = qb - q_start;  // steps; step k handles patch row q_start + k
+  if (warp < kProducers) {
+    const int pxw = c0 - 1 + warp;  // this warp's patch column
+    const bool col_ok = pxw >= 0 && pxw < c1;
+    for (int k = 0; k < K; ++k) {
+      if (k >= 2) bar_sync(kBarEmpty + (k & 1));  // slot k % 3 released by step k - 2
+      if (col_ok)
+        filter_patch(a1, a2, phi, S.ring + (k % kRing) * kSlot + warp * kP * kPitch, g, ay.o0, ax.o0, q_start + k,
+                     pxw, alpha, lane);
+      bar_arrive(kBarFull + (k & 1));
+    }
+    return;
+  }
+  const int ov2 = 2 * g.ov, nx = (c1 - c0) * g.s;
+  const int cw = warp - kProducers;
+  for (int k = 0; k < K; ++k) {
+    bar_sync(kBarFull + (k & 1));  // patch row q_start + k filtered
+    const int q = q_start + k;
+    if (q >= qa) {
+      // tile rows [q s - ov, (q + 1) s - ov): patch row q at offset ry (slot
+      // k % 3) and q - 1 at ry + s for ry < 2 ov (slot (k - 1) % 3); slot 0 of
+      // the parity order is the even row
+      const float2* cur = S.ring + (k % kRing) * kSlot;
+      const float2* prv = S.ring + ((k + kRing - 1) % kRing) * kSlot;
       const bool odd = q & 1;
-      for (int ry = warp; ry < g.s; ry += kFusedWarps) {
+      for (int ry = cw; ry < g.s; ry += kConsumers) {
         const int ty = q * g.s - g.ov + ry;
         const int y = axis_out(ay, ty, g.H, g);
         if (y < 0) continue;
@@ -420,34 +459,67 @@ __global__ void __launch_bounds__(32 * kFusedWarps, 2)
         const float f_own = pack_factor(ry, ty, g.ov, g.sub);
         const float f_oth = (q >= 1 && ry < ov2) ? pack_factor(ry + g.s, ty, g.ov, g.sub) : 0.0f;
         const float fy0 = odd ? f_oth : f_own, fy1 = odd ? f_own : f_oth;
-        const int rc = ry * kPitch, rp = ry * kP;
+        const float2* row0 = odd ? prv + (ry + g.s) * kPitch : cur + ry * kPitch;
+        const float2* row1 = odd ? cur + ry * kPitch : prv + (ry + g.s) * kPitch;
         for (int cxr = lane; cxr < nx; cxr += 32) {
-          const int x = t_xo[cxr];
+          const int x = S.t_xo[cxr];
           if (x < 0) continue;
-          float2 v = raw_z(a1, a2, phi, irow + t_icol[cxr]);
+          float2 v = raw_z(a1, a2, phi, irow + S.t_icol[cxr]);
 #pragma unroll
           for (int xpar = 0; xpar < 2; ++xpar) {
-            const float fx = t_fx[xpar * kMaxNx + cxr];
+            const float fx = S.t_fx[xpar * kMaxNx + cxr];
             if (fx == 0.0f) continue;
-            const int cb = t_cb[xpar * kMaxNx + cxr] + rc, pb = t_pb[xpar * kMaxNx + cxr] + rp;
-            if (fy0 != 0.0f) add_sample(v, fx, fy0, odd ? prev[pb] : cur[cb]);
-            if (fy1 != 0.0f) add_sample(v, fx, fy1, odd ? cur[cb] : prev[pb]);
+            const int cb = S.t_cb[xpar * kMaxNx + cxr];
+            if (fy0 != 0.0f) add_sample(v, fx, fy0, row0[cb]);
+            if (fy1 != 0.0f) add_sample(v, fx, fy1, row1[cb]);
           }
           write_polar(ref, phase, (size_t)y * g.W + x, v);
         }
       }
     }
-    __syncthreads();  // every read of cur and prev done
-    // keep the last 2 ov rows of this patch row for the next one
-    if (col_ok)
-      for (int k = lane; k < ov2 * kP; k += 32) myprev[k] = mycur[(g.s + (k >> 5)) * kPitch + (k & 31)];
-    __syncwarp();
+    if (k + 2 < K) bar_arrive(kBarEmpty + (k & 1));  // done with slots k % 3 and (k - 1) % 3
   }
 }
 
-size_t goldstein_fused_smem(int ov) {
-  return ((size_t)kFusedWarps * kP * kPitch + (size_t)kFusedWarps * 2 * ov * kP) * sizeof(float2) +
-         (size_t)8 * kMaxNx * sizeof(int);
+// The work of a tile is strips x rows patch-row steps (rows = the main patch
+// rows plus the far one), strip-major; CTA b of G resident ones takes steps
+// [b T / G, (b + 1) T / G), so every CTA gets the same work in one wave.
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    goldstein_fused_kernel(const float* __restrict__ a1, const float* __restrict__ a2,
+                           const float* __restrict__ phi, float* __restrict__ ref, float* __restrict__ phase,
+                           GoldsteinGeom g, GoldsteinAxis ay, GoldsteinAxis ax, float alpha) {
+  extern __shared__ float2 gsm[];
+  FusedSmem S;
+  S.ring = gsm;
+  S.t_xo = reinterpret_cast<int*>(gsm + kRing * kSlot);
+  S.t_icol = S.t_xo + kMaxNx;
+  S.t_cb = S.t_icol + kMaxNx;
+  S.t_fx = reinterpret_cast<float*>(S.t_cb + 2 * kMaxNx);
+  const int rows = ay.n_main + (ay.q_far >= 0 ? 1 : 0);
+  const long long T = (long long)ax.groups * rows;
+  const long long u0 = T * blockIdx.x / gridDim.x, u1 = T * (blockIdx.x + 1) / gridDim.x;
+  for (long long u = u0; u < u1;) {
+    const int strip = (int)(u / rows);
+    const int j0 = (int)(u - (long long)strip * rows);
+    const int j1 = (int)min((long long)rows, u1 - (long long)strip * rows);
+    u = (long long)strip * rows + j1;
+    int c0, c1;
+    axis_range(ax, strip, kStripX, c0, c1);
+    __syncthreads();  // the previous run's ring and tables are no longer read
+    fused_tables(S, g, ax, c0, c1);
+    __syncthreads();
+    // steps j < n_main are patch rows q_lo + j, step n_main the far one
+    const int jm = min(j1, ay.n_main);
+    if (j0 < jm) fused_run(a1, a2, phi, ref, phase, S, g, ay, ax, alpha, c0, c1, ay.q_lo + j0, ay.q_lo + jm);
+    if (j1 > ay.n_main) {
+      __syncthreads();
+      fused_run(a1, a2, phi, ref, phase, S, g, ay, ax, alpha, c0, c1, ay.q_far, ay.q_far + 1);
+    }
+  }
+}
+
+size_t goldstein_fused_smem() {
+  return (size_t)kRing * kSlot * sizeof(float2) + (size_t)6 * kMaxNx * sizeof(int);
 }
 
 // patches (of the n per side) covering tile positions [lo, hi]
@@ -548,18 +620,25 @@ int goldstein_device(const float* a1, const float* a2, const float* phi, float* 
   rc = ensure_device_ready(dev);
   if (rc) return rc;
   const std::vector<GoldsteinTile> tiles = goldstein_tiles(g);
-  if (!g_goldstein_two_pass) {
-    const size_t smem = goldstein_fused_smem(ov);
+  if (g_goldstein_fused) {
+    const size_t smem = goldstein_fused_smem();
     static size_t allowed[kMaxDevices];
-    cudaError_t e = allow_dynamic_smem((const void*)goldstein_fused_kernel, goldstein_fused_smem(kMaxOv2 / 2), allowed);
+    cudaError_t e = allow_dynamic_smem((const void*)goldstein_fused_kernel, smem, allowed);
     if (e != cudaSuccess) return cuda_error(e, "Goldstein shared memory");
+    int sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, goldstein_fused_kernel, kFusedThreads, smem);
+    if (e != cudaSuccess) return cuda_error(e, "Goldstein occupancy");
+    const long long resident = (long long)std::max(per_sm, 1) * sms;
     // tiles own disjoint outputs: one launch each (one for most scenes)
     for (const GoldsteinTile& t : tiles) {
-      const GoldsteinAxis ay = goldstein_axis(g, t.h0, t.y_lo, t.y_hi, H, kBandRows);
+      const GoldsteinAxis ay = goldstein_axis(g, t.h0, t.y_lo, t.y_hi, H, 1);
       const GoldsteinAxis ax = goldstein_axis(g, t.w0, t.x_lo, t.x_hi, W, kStripX);
-      if (ay.groups == 0 || ax.groups == 0) continue;
-      goldstein_fused_kernel<<<dim3(ax.groups, ay.groups), 32 * kFusedWarps, smem, st>>>(a1, a2, phi, ref, phase, g,
-                                                                                        ay, ax, alpha);
+      const long long steps = (long long)ax.groups * (ay.n_main + (ay.q_far >= 0 ? 1 : 0));
+      if (steps == 0) continue;
+      const unsigned grid = (unsigned)std::min(steps, resident);
+      goldstein_fused_kernel<<<grid, kFusedThreads, smem, st>>>(a1, a2, phi, ref, phase, g, ay, ax, alpha);
       profile_count(1);
     }
     e = cudaGetLastError();

@@ -76,7 +76,8 @@ from despeckcl_b200 import synthetic
 out = []
 for (H, W, ov, alpha, seed) in [(48, 48, 4, 0.5, 1), (100, 73, 4, 0.5, 2), (257, 300, 4, 0.5, 3), (64, 200, 7, 0.3, 4),
                                 (90, 130, 2, 0.8, 5), (700, 100, 4, 0.5, 6), (1, 1, 4, 0.5, 7), (5, 3, 0, 0.5, 8),
-                                (33, 500, 5, 0.0, 9), (1000, 1000, 4, 0.5, 10)]:
+                                (33, 500, 5, 0.0, 9), (1000, 1000, 4, 0.5, 10), (61, 40, 4, 0.5, 11),
+                                (85, 85, 4, 0.5, 12), (997, 997, 4, 0.5, 13), (37, 19, 4, 0.5, 14)]:
     a1, a2, ph = synthetic.insar_scene(H, W, seed)
     r, p, _ = dcl.goldstein(a1, a2, ph, 32, ov, alpha)
     out += [r, p]
@@ -85,20 +86,21 @@ np.savez(os.environ["DCL_OUT"], *out)
 
 
 def test_fused_kernel_equals_two_pass_path_bit_for_bit(tmp_path):
-    # the fused kernel (patches kept in shared memory) and the two-kernel path
-    # (patches through HBM) run the same FFT, weighting and parity-ordered
-    # overlap-add, so they agree exactly; scenes include non-square ones whose
-    # last row or column lies in a separate strip or band, overlaps 0..7 and
-    # alpha 0
+    # the fused kernel (DESPECKCL_B200_GOLDSTEIN_FUSED=1, patches kept in
+    # shared memory) and the default two-kernel path (patches through HBM) run
+    # the same FFT, weighting and parity-ordered overlap-add, so they agree
+    # exactly; scenes include non-square ones, ones whose last row or column
+    # comes from a second reference tile (61 x 40, 85 x 85, 997 x 997, 37 x 19),
+    # overlaps 0..7 and alpha 0
     import os
     import subprocess
     import sys
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     res = []
-    for name, two in (("fused", "0"), ("two", "1")):
+    for name, fused in (("fused", "1"), ("two", "0")):
         env = dict(os.environ, DCL_ROOT=root, DCL_OUT=str(tmp_path / f"{name}.npz"),
-                   DESPECKCL_B200_GOLDSTEIN_TWO_PASS=two)
+                   DESPECKCL_B200_GOLDSTEIN_FUSED=fused)
         r = subprocess.run([sys.executable, "-c", FUSED_VS_TWO_PASS], env=env, capture_output=True, text=True,
                            timeout=600)
         assert r.returncode == 0, r.stderr[-3000:]
