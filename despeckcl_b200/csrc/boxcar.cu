@@ -17,6 +17,7 @@
 
 #include "../../include/despeckcl_b200.h"
 #include "dcl_internal.h"
+#include "fast_math.cuh"
 
 namespace dcl {
 namespace {
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(kBoxThreads)
     }
     const size_t o = (size_t)oy * W + ox;
     ref[o] = si * inv_n;
-    phase[o] = atan2f(sj, sr);
+    phase[o] = atan2_fast(sj, sr);
     coh[o] = sqrtf(sr * sr + sj * sj) / si;
   }
 }
@@ -142,28 +143,65 @@ __global__ void __launch_bounds__(kBoxThreads)
   // staging: each thread issues the loads of U pixels (all of its share, up
   // to 12) before using any of them, so up to 3U loads per thread are in
   // flight (the staging is bound by memory latency, not bandwidth, at one
-  // load in flight per plane)
+  // load in flight per plane).  A thread's staged pixels are i = tid + u T
+  // (T threads); their (row, column) advance by (T / SW, T % SW) with one
+  // carry, with no division.  Tiles whose staged region lies inside the
+  // scene (all but the edge tiles) read without clamping, at 32-bit offsets
+  // from the tile's first staged pixel.
   constexpr int U = (SH * SW + kBoxThreads - 1) / kBoxThreads < 12 ? (SH * SW + kBoxThreads - 1) / kBoxThreads : 12;
+  constexpr int DR = (U * kBoxThreads) / SW, DC = (U * kBoxThreads) % SW;
+  constexpr int dr = kBoxThreads / SW, dc = kBoxThreads % SW;
+  const bool interior = vy0 >= R && vy0 + kBoxTH + R <= H && vx0 >= R && vx0 + kBoxTW + R <= W;
+  const size_t base = interior ? (size_t)(vy0 - R) * W + (vx0 - R) : 0;
+  const float* b1 = a1 + base;
+  const float* b2 = a2 + base;
+  const float* bp = phi + base;
+  int rr0 = tid / SW, cc0 = tid - (tid / SW) * SW;
   for (int i0 = tid; i0 < SH * SW; i0 += U * kBoxThreads) {
     float am[U], as[U], ph[U];
+    int sidx[U];
+    {
+      int rr = rr0, cc = cc0;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * kBoxThreads;
-      if (i < SH * SW) {
-        const int rr = i / SW, cc = i - rr * SW;
-        const int y = clampi_b(vy0 - R + rr, 0, H - 1), x = clampi_b(vx0 - R + cc, 0, W - 1);
-        const size_t g = (size_t)y * W + x;
-        am[u] = __ldg(a1 + g);
-        as[u] = __ldg(a2 + g);
-        ph[u] = __ldg(phi + g);
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + u * kBoxThreads;
+        if (i < SH * SW) {
+          int off;
+          if (interior) {
+            off = rr * W + cc;
+          } else {
+            const int y = clampi_b(vy0 - R + rr, 0, H - 1), x = clampi_b(vx0 - R + cc, 0, W - 1);
+            off = 0;
+            am[u] = __ldg(a1 + (size_t)y * W + x);
+            as[u] = __ldg(a2 + (size_t)y * W + x);
+            ph[u] = __ldg(phi + (size_t)y * W + x);
+          }
+          if (interior) {
+            am[u] = __ldg(b1 + off);
+            as[u] = __ldg(b2 + off);
+            ph[u] = __ldg(bp + off);
+          }
+          sidx[u] = rr * SWP + cc;
+        }
+        rr += dr;
+        cc += dc;
+        if (cc >= SW) {
+          cc -= SW;
+          ++rr;
+        }
       }
+    }
+    rr0 += DR;
+    cc0 += DC;
+    if (cc0 >= SW) {
+      cc0 -= SW;
+      ++rr0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = i0 + u * kBoxThreads;
       if (i < SH * SW) {
-        const int rr = i / SW;
-        const int si = i + rr * (SWP - SW);
+        const int si = sidx[u];
         float sn, cs;
         __sincosf(ph[u], &sn, &cs);
         const float aa = am[u] * as[u];
@@ -219,7 +257,7 @@ __global__ void __launch_bounds__(kBoxThreads)
       const float si = sum[0][q], sr = sum[1][q], sj = sum[2][q];
       const size_t o = (size_t)oy * W + ox;
       ref[o] = si * inv_n;
-      phase[o] = atan2f(sj, sr);
+      phase[o] = atan2_fast(sj, sr);
       // |sum| / sum I with the hardware square root and the fast division
       // (a few ulps, against the 1e-4 relative tolerance of the coherence):
       // 6 % of the kernel's time at w 7 against the correctly rounded pair

@@ -50,6 +50,7 @@
 
 #include "../../include/despeckcl_b200.h"
 #include "dcl_internal.h"
+#include "fast_math.cuh"
 
 namespace dcl {
 namespace {
@@ -243,10 +244,10 @@ __device__ __forceinline__ void add_sample(float2& v, float fx, float fy, float2
   v.y = __fmaf_rn(f, q.y, v.y);
 }
 
-// |Z| and arg Z (slc2real.cl)
+// |Z| and arg Z (slc2real.cl); the angle within 6e-7 rad (atan2_fast)
 __device__ __forceinline__ void write_polar(float* __restrict__ ref, float* __restrict__ phase, size_t o, float2 v) {
   ref[o] = fabsf(sqrtf(__fmaf_rn(v.x, v.x, __fmul_rn(v.y, v.y))));
-  phase[o] = atan2f(v.y, v.x);
+  phase[o] = atan2_fast(v.y, v.x);
 }
 
 constexpr int kPackX = 4;  // output columns per thread (32 apart: coalesced per warp)

@@ -7,10 +7,14 @@
 // Per CTA: a 32 x 32 output tile (32 x 24 for 8-plane covariance input), each
 // thread owning 2 (16 warps) or 4 (8 warps) vertically consecutive pixels of
 // one column.  For every scale the search-window offsets are taken three at a
-// time (seven when every pass has one patch size of at most 7) along a row of the window (same
-// dy, consecutive dx, so a thread's neighbour loads overlap across the batch):
-//   A  GLR similarities of the batch on the tile plus the patch halo
-//      (each thread: one pixel x three offsets); the measure is evaluated in
+// time (seven when every pass has one patch size of at most 7) along a row of
+// the window (same dy, consecutive dx), in the reference's summation order
+// (row-major over the window, compute_nl_statistics.cl:77-78):
+//   A  GLR similarities of the batch on the tile plus the patch halo (three
+//      offsets: each thread three adjacent columns of one row, the neighbour
+//      of column j at offset k being neighbour column j + k, so five
+//      neighbour loads serve nine pairs; seven offsets: each thread one pixel
+//      x the seven offsets); the measure is evaluated in
 //      an order symmetric in its two pixels, so the mirrored half window gets
 //      exactly the values of the reference's copy
 //      (center first in the upper half, neighbour first in the mirrored half,
@@ -199,6 +203,14 @@ __device__ __forceinline__ float pixel_term(const float4 c) {
   return d >= 0.0f ? __fdiv_rn(0.25f, fabsf(d)) : __int_as_float(0x7fffffff);
 }
 
+// load of one float from a 32-bit shared-memory address, for tables that
+// stay unchanged while they are read (the compiler may schedule it freely)
+__device__ __forceinline__ float lds_f32(uint32_t addr) {
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+
 __device__ __forceinline__ float lg2_ftz(float x) {
   float y;
   asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -252,7 +264,7 @@ struct Best {
 // combinations update the selection state.  The staged scaled covariance
 // carries the halo of the call's largest patch; a pass with smaller patches
 // reads its region CO pixels further in.
-template <class L, int PH0, int PH1, int PH2, int PV>
+template <class L, int PH0, int PH1, int PH2, int PV, bool HT>
 __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParams& pp, float* smem,
                                           Best<L::PX, L::NM>& best) {
   constexpr int WSH = L::WSH, K = L::K, RS = L::RS, RO = L::RO, TW = L::TW, PX = L::PX;
@@ -297,10 +309,19 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
       dmax[j] *= 1.44269504f;
     }
   }
-  // this lane's copy of the table of component j
+  // shared-memory address of this lane's copy of the table of component j,
+  // less the 2^23 bias of the index float's bits times the entry stride:
+  // adding those bits times the stride gives the entry's address (32-bit
+  // shared addresses wrap modulo 2^32), one instruction fewer per lookup
+  // (the 8-plane instantiations, at their register limit, index this lane's
+  // copy as an array instead)
+  uint32_t lut_a[NP];
   const float* lut_j[NP];
 #pragma unroll
-  for (int j = 0; j < NP; ++j) lut_j[j] = sLut + j * kMaxLut * L::LUTREP + (lane & (L::LUTREP - 1));
+  for (int j = 0; j < NP; ++j) {
+    lut_j[j] = sLut + j * kMaxLut * L::LUTREP + (lane & (L::LUTREP - 1));
+    lut_a[j] = smem_u32(lut_j[j]) - 0x4B000000u * (4u * L::LUTREP);
+  }
   float2 acc[PX / 2][NP][NA];  // .x: pixel 2i, .y: pixel 2i+1
   constexpr int NKC = PV == kPrecKahan ? NA : 1;  // Kahan compensation terms
   float2 kc[PX / 2][NP][NKC];
@@ -317,19 +338,57 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
 
   for (int dy = -WSH; dy <= WSH; ++dy) {
     for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
-      // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
-      // thread and consecutive pixels on consecutive lanes (conflict free)
-      // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-      for (int it = tid; it < SIMH * SIMP; it += NT) {
-        const int r = it / SIMP;
-        const int c = it - r * SIMP;
-        if (c >= SIMW) continue;
-        const int ci = (r + WSH + CO) * RS + (c + WSH + CO);
-        const float4 a = sCs[ci];
-        const float la = sLd[ci];
-        const int ni = ci + dy * RS + dx0;
+      if constexpr (HT) {
+        // ---- A, column triples: a thread takes three adjacent columns of
+        // one row of the similarity region for the three offsets; the
+        // neighbour of column j at offset k is neighbour column j + k, so
+        // three centre and five neighbour loads serve the nine pairs.
+        // Consecutive lanes take consecutive triples: their 16-byte loads
+        // (stride 48 bytes) and 4-byte stores (stride 3 words) are conflict
+        // free.  The last triple of a row holds its last one or two columns
+        // where the width is not a multiple of three; loads for its missing
+        // columns repeat its last needed one, so every index stays inside the
+        // staged region.
+        constexpr int NTC = (SIMW + 2) / 3;
+        for (int it = tid; it < SIMH * NTC; it += NT) {
+          const int r = it / NTC;
+          const int c0 = 3 * (it - r * NTC);
+          const int nc = SIMW - c0 < 3 ? SIMW - c0 : 3;
+          const int ci = (r + WSH + CO) * RS + (c0 + WSH + CO);
+          const int ni = ci + dy * RS + dx0;
+          float4 b[K + 2];
+          float lb[K + 2];
 #pragma unroll
-        for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim<PV>(a, la, sCs[ni + k], sLd[ni + k], c2d);
+          for (int j = 0; j < K + 2; ++j) {
+            const int nj = ni + (j < nc + K - 1 ? j : nc + K - 2);
+            b[j] = sCs[nj];
+            lb[j] = sLd[nj];
+          }
+          float* out = sSim + r * SIMP + c0;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            if (j >= nc) break;
+            const float4 a = sCs[ci + j];
+            const float la = sLd[ci + j];
+#pragma unroll
+            for (int k = 0; k < K; ++k) out[k * SIMH * SIMP + j] = glr_sim<PV>(a, la, b[j + k], lb[j + k], c2d);
+          }
+        }
+      } else {
+        // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
+        // thread and consecutive pixels on consecutive lanes (conflict free)
+        // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
+        for (int it = tid; it < SIMH * SIMP; it += NT) {
+          const int r = it / SIMP;
+          const int c = it - r * SIMP;
+          if (c >= SIMW) continue;
+          const int ci = (r + WSH + CO) * RS + (c + WSH + CO);
+          const float4 a = sCs[ci];
+          const float la = sLd[ci];
+          const int ni = ci + dy * RS + dx0;
+#pragma unroll
+          for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim<PV>(a, la, sCs[ni + k], sLd[ni + k], c2d);
+        }
       }
       __syncthreads();
       // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
@@ -424,8 +483,12 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
               // index; d > dmax has weight 0
               const float u = __saturatef(fmaf(d, inv_span[j], nbias[j]));
               const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
-              const int idx = __float_as_int(t) - 0x4B000000;
-              const float lw = lut_j[j][idx * L::LUTREP];
+              float lw;
+              if constexpr (FULL8) {
+                lw = lut_j[j][(__float_as_int(t) - 0x4B000000) * L::LUTREP];
+              } else {
+                lw = lds_f32(lut_a[j] + static_cast<uint32_t>(__float_as_int(t)) * (4u * L::LUTREP));
+              }
               w[i][j] = (d > dmax[j]) ? 0.0f : lw;
             }
           }
@@ -551,6 +614,9 @@ template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int 
 __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
   using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
+  // phase A in column triples wherever a batch holds three offsets of InSAR
+  // input (the 8-plane instantiations are at their register limit)
+  constexpr bool HT = L::K == 3 && !L::FULL8;
   constexpr int RS = L::RS, RSH = L::RSH, RO = L::RO, TW = L::TW, PX = L::PX;
   constexpr int NT = L::THREADS, NM = L::NM;
   constexpr bool FULL8 = L::FULL8;
@@ -626,12 +692,12 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
         loaded_slot = pp.scale_slot;
       }
       if constexpr (B0 < 0) {
-        fast_pass<L, A0, A1, A2, PV>(P, pp, smem, best);
+        fast_pass<L, A0, A1, A2, PV, HT>(P, pp, smem, best);
       } else {
         if (pass_is<A0, A1, A2>(pp))
-          fast_pass<L, A0, A1, A2, PV>(P, pp, smem, best);
+          fast_pass<L, A0, A1, A2, PV, HT>(P, pp, smem, best);
         else
-          fast_pass<L, B0, B1, B2, PV>(P, pp, smem, best);
+          fast_pass<L, B0, B1, B2, PV, HT>(P, pp, smem, best);
       }
     }
 

@@ -20,7 +20,10 @@
 //    at zero, but all calls on one device share the array: calls that overlap
 //    on the GPU (different streams or threads at the same time) race;
 //  * the first call on a device resolves the array's device address
-//    (cudaGetSymbolAddress); make that first call before any stream capture.
+//    (cudaGetSymbolAddress); make that first call before any stream capture;
+//  * the scene descriptor and weight tables are copied from pageable host
+//    memory, so a call may wait for the stream's earlier work before it
+//    returns.
 
 #include <cuda_runtime.h>
 
