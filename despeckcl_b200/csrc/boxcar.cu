@@ -15,6 +15,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "../../include/despeckcl_b200.h"
 #include "dcl_internal.h"
 #include "fast_math.cuh"
@@ -91,53 +93,89 @@ __global__ void __launch_bounds__(kBoxThreads)
   }
 }
 
+// Packed and scalar adds for the window sums: (Re, Im) pairs are summed two
+// lanes at a time with the f32x2 add (each component rounded like a scalar
+// add).
+__device__ __forceinline__ float wadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float2 wadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
 // Window sums of 4 consecutive outputs o[q] = v[q] + ... + v[q + w - 1],
 // q = 0..3, from the 4 + w - 1 values v: the part v[3 .. w-1] that all four
 // windows share is added once, then each window adds its own ends (w + 6 adds
 // instead of 4 w).  No term is subtracted, so no sum cancels.
-template <int R>
-__device__ __forceinline__ void window4(const float* v, float* o) {
+template <int R, class T>
+__device__ __forceinline__ void window4(const T* v, T* o) {
   constexpr int w = 2 * R + 1;
   if (w < 4) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      float acc = v[q];
+      T acc = v[q];
 #pragma unroll
-      for (int k = 1; k < w; ++k) acc += v[q + k];
+      for (int k = 1; k < w; ++k) acc = wadd(acc, v[q + k]);
       o[q] = acc;
     }
     return;
   }
-  float c = v[3];
+  T c = v[3];
 #pragma unroll
-  for (int k = 4; k < w; ++k) c += v[k];
-  const float l1 = v[1] + v[2];
-  const float l0 = v[0] + l1;
-  const float r2 = v[w] + v[w + 1];
-  const float r3 = r2 + v[w + 2];
-  o[0] = l0 + c;
-  o[1] = (l1 + c) + v[w];
-  o[2] = (v[2] + c) + r2;
-  o[3] = c + r3;
+  for (int k = 4; k < w; ++k) c = wadd(c, v[k]);
+  const T l1 = wadd(v[1], v[2]);
+  const T l0 = wadd(v[0], l1);
+  const T r2 = wadd(v[w], v[w + 1]);
+  const T r3 = wadd(r2, v[w + 2]);
+  o[0] = wadd(l0, c);
+  o[1] = wadd(wadd(l1, c), v[w]);
+  o[2] = wadd(wadd(v[2], c), r2);
+  o[3] = wadd(c, r3);
 }
 
-// Compile-time window radius R (w = 2R+1 <= 15): a 64 x 32 tile per CTA,
-// window sums from registers, each thread producing 4 consecutive outputs
-// (columns in the horizontal pass, rows in the vertical one) from 4 + 2R
-// loaded values per plane, with the shared part of their windows summed once
-// (window4).
+// Window sums of 2 consecutive outputs from the w + 1 values v: the middle
+// v[1 .. w-1] is summed once (w + 1 adds instead of 2 (w - 1)).
+template <int R, class T>
+__device__ __forceinline__ void window2(const T* v, T& o0, T& o1) {
+  constexpr int w = 2 * R + 1;
+  if (w == 1) {
+    o0 = v[0];
+    o1 = v[1];
+    return;
+  }
+  T m = v[1];
+#pragma unroll
+  for (int k = 2; k < w; ++k) m = wadd(m, v[k]);
+  o0 = wadd(v[0], m);
+  o1 = wadd(m, v[w]);
+}
+
+// Compile-time window radius R (w = 2R+1 <= 15): a 64 x 32 tile per CTA of
+// 256 threads.  The staged tile holds the intensity I as one plane and the
+// interferogram (Re, Im) as interleaved pairs, so both complex window sums
+// run as packed f32x2 adds:
+//   horizontal pass: window4 over one row x 4 columns of I and window2 over
+//     one row x 2 columns of (Re, Im), from 16-byte loads;
+//   vertical pass, 4 rows x 2 columns per thread (the 256 items of a tile):
+//     window4 down the column pair of I and down each column's (Re, Im),
+//     all as packed adds, from 8- and 16-byte loads;
+//   output: ref = mean I, phase = atan2(Im, Re), coh = |sum| / sum I, written
+//     as 8-byte vectors where both columns are interior and the planes allow
+//     it.
 template <int R>
 __global__ void __launch_bounds__(kBoxThreads)
     boxcar_r_kernel(const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ phi,
-                    float* __restrict__ ref, float* __restrict__ phase, float* __restrict__ coh, int H, int W) {
+                    float* __restrict__ ref, float* __restrict__ phase, float* __restrict__ coh, int H, int W,
+                    int vec_out) {
   // staged rows of SW values, pitch SWP (a multiple of 4: the horizontal
   // pass reads its windows as aligned 16-byte vectors, conflict free)
   constexpr int SW = kBoxTW + 2 * R, SH = kBoxTH + 2 * R, N = 4 + 2 * R;
   constexpr int SWP = (SW + 3) / 4 * 4, NQ = (N + 3) / 4;
-  static_assert(4 * (kBoxTW / 4 - 1) + 4 * NQ <= SWP, "window vectors stay inside a staged row");
+  constexpr int HG = kBoxTW / 4;
+  static_assert(4 * (HG - 1) + 4 * NQ <= SWP && (kBoxTW - 2) + 2 * (R + 1) <= SWP,
+                "window vectors stay inside a staged row");
+  static_assert((kBoxTH / 4) * (kBoxTW / 2) == kBoxThreads, "one vertical item per thread");
   extern __shared__ __align__(16) float sm[];
-  float* sIn = sm;                   // [3][SH][SWP]: I, Re, Im
-  float* sHs = sm + 3 * SH * SWP;    // [3][SH][kBoxTW] horizontal sums
+  float* sI = sm;                                              // [SH][SWP]
+  float2* sZ = reinterpret_cast<float2*>(sm + SH * SWP);        // [SH][SWP] (Re, Im)
+  float* hI = sm + 3 * SH * SWP;                               // [SH][kBoxTW] horizontal sums
+  float2* hZ = reinterpret_cast<float2*>(hI + SH * kBoxTW);     // [SH][kBoxTW]
   const int vy0 = blockIdx.y * kBoxTH, vx0 = blockIdx.x * kBoxTW;
   const int tid = threadIdx.x;
   // staging: each thread issues the loads of U pixels (all of its share, up
@@ -205,65 +243,106 @@ __global__ void __launch_bounds__(kBoxThreads)
         float sn, cs;
         __sincosf(ph[u], &sn, &cs);
         const float aa = am[u] * as[u];
-        sIn[si] = (am[u] * am[u] + as[u] * as[u]) / 2;
-        sIn[SH * SWP + si] = aa * cs;
-        sIn[2 * SH * SWP + si] = aa * sn;
+        sI[si] = (am[u] * am[u] + as[u] * as[u]) / 2;
+        sZ[si] = make_float2(aa * cs, aa * sn);
       }
     }
   }
   __syncthreads();
-  // horizontal: item = (plane, row, group of 4 columns)
-  constexpr int HG = kBoxTW / 4;
-  for (int it = tid; it < 3 * SH * HG; it += kBoxThreads) {
-    const int pl = it / (SH * HG);
-    const int rem = it - pl * SH * HG;
-    const int rr = rem / HG, c0 = (rem - rr * HG) * 4;
-    const float4* src = reinterpret_cast<const float4*>(sIn + pl * SH * SWP + rr * SWP + c0);
-    float v[4 * NQ];
+  // horizontal: items of I (row, 4 columns: window4 from 16-byte loads) and
+  // of (Re, Im) (row, 2 columns: window2 from 16-byte loads of 2 pairs);
+  // consecutive lanes read consecutive 16-byte vectors of one row
+  constexpr int NI = SH * HG, NZ = SH * (kBoxTW / 2);
+  for (int it = tid; it < NI + NZ; it += kBoxThreads) {
+    if (it < NI) {
+      const int rr = it / HG, c0 = (it - rr * HG) * 4;
+      const float4* src = reinterpret_cast<const float4*>(sI + rr * SWP + c0);
+      float v[4 * NQ];
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      const float4 t = src[q];
-      v[4 * q] = t.x;
-      v[4 * q + 1] = t.y;
-      v[4 * q + 2] = t.z;
-      v[4 * q + 3] = t.w;
+      for (int q = 0; q < NQ; ++q) {
+        const float4 t = src[q];
+        v[4 * q] = t.x;
+        v[4 * q + 1] = t.y;
+        v[4 * q + 2] = t.z;
+        v[4 * q + 3] = t.w;
+      }
+      float o[4];
+      window4<R>(v, o);
+      *reinterpret_cast<float4*>(hI + rr * kBoxTW + c0) = make_float4(o[0], o[1], o[2], o[3]);
+    } else {
+      const int j = it - NI;
+      const int rr = j / (kBoxTW / 2), c0 = (j - rr * (kBoxTW / 2)) * 2;
+      const float4* src = reinterpret_cast<const float4*>(sZ + rr * SWP + c0);
+      float2 v[2 + 2 * R + 1];
+#pragma unroll
+      for (int q = 0; q < R + 1; ++q) {
+        const float4 t = src[q];
+        v[2 * q] = make_float2(t.x, t.y);
+        v[2 * q + 1] = make_float2(t.z, t.w);
+      }
+      float2 o0, o1;
+      window2<R>(v, o0, o1);
+      *reinterpret_cast<float4*>(hZ + rr * kBoxTW + c0) = make_float4(o0.x, o0.y, o1.x, o1.y);
     }
-    float o[4];
-    window4<R>(v, o);
-    *reinterpret_cast<float4*>(sHs + pl * SH * kBoxTW + rr * kBoxTW + c0) = make_float4(o[0], o[1], o[2], o[3]);
   }
   __syncthreads();
-  // vertical: item = (group of 4 rows, column); all three planes
-  const float inv_n = 1.0f / (float)((2 * R + 1) * (2 * R + 1));
-  for (int it = tid; it < (kBoxTH / 4) * kBoxTW; it += kBoxThreads) {
-    const int r0 = (it / kBoxTW) * 4, cc = it - (it / kBoxTW) * kBoxTW;
-    float sum[3][4];
+  // vertical: this thread's 4 rows x 2 columns (a warp covers 4 rows of the
+  // tile's 64 columns): window4 down the column pair of I and down each
+  // column's (Re, Im), all as packed adds
+  const int c0 = (tid % (kBoxTW / 2)) * 2, r0 = (tid / (kBoxTW / 2)) * 4;
+  float2 sIp[4];     // [row]: (I of column c0, I of column c0 + 1)
+  float2 sZc[2][4];  // [column][row]: (Re, Im)
+  {
+    float2 vi[N], vz0[N], vz1[N];
 #pragma unroll
-    for (int pl = 0; pl < 3; ++pl) {
-      const float* src = sHs + pl * SH * kBoxTW + r0 * kBoxTW + cc;
-      float v[N];
-#pragma unroll
-      for (int k = 0; k < N; ++k) v[k] = src[k * kBoxTW];
-      window4<R>(v, sum[pl]);
+    for (int k = 0; k < N; ++k) {
+      vi[k] = *reinterpret_cast<const float2*>(hI + (r0 + k) * kBoxTW + c0);
+      const float4 t = *reinterpret_cast<const float4*>(hZ + (r0 + k) * kBoxTW + c0);
+      vz0[k] = make_float2(t.x, t.y);
+      vz1[k] = make_float2(t.z, t.w);
     }
-    const int vx = vx0 + cc;
-    const int ox = (vx < W - 1) ? vx : (vx == W - 1 + R ? W - 1 : -1);
-    if (ox < 0) continue;
+    window4<R>(vi, sIp);
+    window4<R>(vz0, sZc[0]);
+    window4<R>(vz1, sZc[1]);
+  }
+  // outputs on the virtual plane: row H-1 holds virtual row H-1+R (likewise
+  // column W-1); a column pair wholly left of column W-1 maps to itself
+  const float inv_n = 1.0f / (float)((2 * R + 1) * (2 * R + 1));
+  const int vx = vx0 + c0;
+  const bool cols_plain = vx + 1 < W - 1;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int vy = vy0 + r0 + q;
-      const int oy = (vy < H - 1) ? vy : (vy == H - 1 + R ? H - 1 : -1);
-      if (oy < 0) continue;
-      const float si = sum[0][q], sr = sum[1][q], sj = sum[2][q];
-      const size_t o = (size_t)oy * W + ox;
-      ref[o] = si * inv_n;
-      phase[o] = atan2_fast(sj, sr);
+  for (int q = 0; q < 4; ++q) {
+    const int vy = vy0 + r0 + q;
+    const int oy = (vy < H - 1) ? vy : (vy == H - 1 + R ? H - 1 : -1);
+    if (oy < 0) continue;
+    float o_r[2], o_p[2], o_c[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const float si = e == 0 ? sIp[q].x : sIp[q].y;
+      const float sr = sZc[e][q].x, sj = sZc[e][q].y;
+      o_r[e] = si * inv_n;
+      o_p[e] = atan2_fast(sj, sr);
       // |sum| / sum I with the hardware square root and the fast division
-      // (a few ulps, against the 1e-4 relative tolerance of the coherence):
-      // 6 % of the kernel's time at w 7 against the correctly rounded pair
+      // (a few ulps, against the 1e-4 relative tolerance of the coherence)
       float m;
       asm("sqrt.approx.f32 %0, %1;" : "=f"(m) : "f"(sr * sr + sj * sj));
-      coh[o] = __fdividef(m, si);
+      o_c[e] = __fdividef(m, si);
+    }
+    const size_t rowo = (size_t)oy * W;
+    if (cols_plain && vec_out) {
+      *reinterpret_cast<float2*>(ref + rowo + vx) = make_float2(o_r[0], o_r[1]);
+      *reinterpret_cast<float2*>(phase + rowo + vx) = make_float2(o_p[0], o_p[1]);
+      *reinterpret_cast<float2*>(coh + rowo + vx) = make_float2(o_c[0], o_c[1]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int x = vx + e;
+        const int ox = (x < W - 1) ? x : (x == W - 1 + R ? W - 1 : -1);
+        if (ox < 0) continue;
+        ref[rowo + ox] = o_r[e];
+        phase[rowo + ox] = o_p[e];
+        coh[rowo + ox] = o_c[e];
+      }
     }
   }
 }
@@ -275,7 +354,10 @@ cudaError_t launch_boxcar_r(const float* a1, const float* a2, const float* phi, 
   static size_t allowed[kMaxDevices];
   const cudaError_t e = allow_dynamic_smem((const void*)boxcar_r_kernel<R>, smem, allowed);
   if (e != cudaSuccess) return e;
-  boxcar_r_kernel<R><<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W);
+  // 8-byte output vectors need an even row length and 8-byte aligned planes
+  const int vec_out = (W % 2 == 0) && ((reinterpret_cast<uintptr_t>(ref) | reinterpret_cast<uintptr_t>(phase) |
+                                         reinterpret_cast<uintptr_t>(coh)) % 8 == 0);
+  boxcar_r_kernel<R><<<grid, kBoxThreads, smem, st>>>(a1, a2, phi, ref, phase, coh, H, W, vec_out);
   return cudaGetLastError();
 }
 

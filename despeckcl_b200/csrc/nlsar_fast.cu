@@ -63,16 +63,23 @@ struct FastL {
   static constexpr int K = (NPX == 1 && PHX <= 3) ? 7 : 3;
   static constexpr int NA = FULL8 ? 12 : 8;          // accumulators per (pixel, patch size)
   static constexpr int NM = FULL8 ? 8 : 4;           // weighted sums kept for the selected combination
-  static constexpr int RS = TW + 2 * (PHX + WSH);    // scaled covariance region: RS x RSH
+  // phase A in column triples, one row per lane, where a batch holds three
+  // offsets of InSAR input (fast_pass)
+  static constexpr bool HT = K == 3 && !FULL8;
+  // scaled covariance region: RS x RSH, with one unused pixel more per row
+  // for InSAR input, which makes the row pitch odd (fast_stage)
+  static constexpr int RS = TW + 2 * (PHX + WSH) + (FULL8 ? 0 : 1);
   static constexpr int RSH = TH + 2 * (PHX + WSH);
   static constexpr int RO = TW + 2 * WSH;            // original covariance region: RO x ROH
   static constexpr int ROH = TH + 2 * WSH;
-  // similarity region of the widest pass, SIMWX x SIMHX; its row pitch is a
-  // multiple of 8 words: phase A's lanes write consecutive words, phase B
-  // reads 16-byte vectors, a quarter warp covering 8 consecutive segments of
-  // one row (contiguous, conflict free)
+  // similarity region of the widest pass, SIMWX x SIMHX.  Row pitch: odd
+  // with column triples (phase A's lanes write down a column; phase B's
+  // quarter warps, one row each, then read words of four rows that fall in
+  // different banks), else a multiple of 8 words (phase A's lanes write
+  // consecutive words, phase B reads 16-byte vectors, a quarter warp covering
+  // 8 consecutive segments of one row: contiguous, conflict free)
   static constexpr int SIMWX = TW + 2 * PHX, SIMHX = TH + 2 * PHX;
-  static constexpr int SIMPX = (SIMWX + 7) / 8 * 8;
+  static constexpr int SIMPX = HT ? SIMWX + 1 : (SIMWX + 7) / 8 * 8;
   static constexpr int HP = TW;                      // horizontal-sum row pitch (words), unpadded
   static constexpr int HPL = K * SIMHX * HP;         // one patch size's horizontal-sum plane
   // shared memory, in 4-byte words; the TMA destinations start on 128-byte
@@ -82,7 +89,10 @@ struct FastL {
   static constexpr int OFF_CO2 = (OFF_CO + 4 * RO * ROH + 31) / 32 * 32;  // 8-plane input only
   static constexpr int OFF_H = OFF_CO2 + (FULL8 ? 4 * RO * ROH : 0);
   static constexpr int OFF_LD = OFF_H + NPX * HPL;
-  static constexpr int OFF_SIM = OFF_LD + RS * RSH;
+  // the similarity map starts on a 128-byte boundary: the ln det plane before
+  // it has an odd row pitch for InSAR input, and phase B may read the map in
+  // 16-byte vectors
+  static constexpr int OFF_SIM = (OFF_LD + RS * RSH + 31) / 32 * 32;
   static constexpr int OFF_LUT = OFF_SIM + K * SIMHX * SIMPX;
   // interleaved copies of the composite weight tables: 16 (two lanes per
   // copy) where they fit, else 8 (four lanes per copy)
@@ -92,6 +102,11 @@ struct FastL {
   static constexpr uint32_t CO_BYTES = 16u * RO * ROH;  // one TMA box each
   static constexpr uint32_t CS_BYTES = 16u * RS * RSH;
   static_assert(SWS % K == 0, "offset batches must tile a window row");
+  // every region read or written in 16-byte vectors (or by TMA) starts on a
+  // 16-byte boundary; the mbarrier on an 8-byte one
+  static_assert(OFF_CS % 32 == 0 && OFF_CO % 32 == 0 && OFF_CO2 % 4 == 0 && OFF_H % 4 == 0 && OFF_SIM % 4 == 0 &&
+                    OFF_BAR % 2 == 0,
+                "shared-memory region alignment");
   static_assert(PX % 2 == 0, "pixels are accumulated in pairs");
   static_assert(HP >= TW && HP % 4 == 0, "horizontal-sum pitch");
   static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
@@ -274,10 +289,12 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
   constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
   constexpr int CO = L::PHX - PHM;
   constexpr int SIMW = TW + 2 * PHM, SIMH = L::TH + 2 * PHM;  // this pass's similarity region
-  constexpr int SIMP = (SIMW + 7) / 8 * 8;
+  constexpr int SIMP = HT ? SIMW + 1 : (SIMW + 7) / 8 * 8;  // row pitch (FastL::SIMPX)
   constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
+  static_assert(HT == L::HT && (!HT || K == 3), "column triples serve three offsets");
   static_assert(PH0 >= 0 && NP <= L::NPX && CO >= 0, "pass shape");
-  static_assert(SIMP >= 4 * 7 + 4 * NQ4 && SIMP <= L::SIMPX, "phase-B segments must stay inside a row");
+  static_assert(SIMP <= L::SIMPX && (HT ? SIMP % 2 == 1 : SIMP >= 4 * 7 + 4 * NQ4),
+                "phase-B segments must stay inside a row");
   const float4* sCs = reinterpret_cast<const float4*>(smem + L::OFF_CS);
   const float4* sCo = reinterpret_cast<const float4*>(smem + L::OFF_CO);
   const float4* sCo2 = reinterpret_cast<const float4*>(smem + L::OFF_CO2);  // 8-plane input only
@@ -343,16 +360,20 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
         // one row of the similarity region for the three offsets; the
         // neighbour of column j at offset k is neighbour column j + k, so
         // three centre and five neighbour loads serve the nine pairs.
-        // Consecutive lanes take consecutive triples: their 16-byte loads
-        // (stride 48 bytes) and 4-byte stores (stride 3 words) are conflict
-        // free.  The last triple of a row holds its last one or two columns
-        // where the width is not a multiple of three; loads for its missing
-        // columns repeat its last needed one, so every index stays inside the
-        // staged region.
+        // Consecutive lanes take consecutive rows of one triple of columns:
+        // the staged rows (RS float4) and the similarity rows (SIMP words)
+        // have odd pitches, so their 16-byte loads (8 lanes at a time) and
+        // 4-byte loads and stores (32 lanes) fall in distinct banks.  The
+        // last triple holds the region's last one or two columns where its
+        // width is not a multiple of three; loads for its missing columns
+        // repeat its last needed one, so every index stays inside the staged
+        // region.
         constexpr int NTC = (SIMW + 2) / 3;
+        static_assert(RS % 2 == 1, "odd staged pitch");
         for (int it = tid; it < SIMH * NTC; it += NT) {
-          const int r = it / NTC;
-          const int c0 = 3 * (it - r * NTC);
+          const int tc = it / SIMH;
+          const int r = it - tc * SIMH;
+          const int c0 = 3 * tc;
           const int nc = SIMW - c0 < 3 ? SIMW - c0 : 3;
           const int ci = (r + WSH + CO) * RS + (c0 + WSH + CO);
           const int ni = ci + dy * RS + dx0;
@@ -402,15 +423,22 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
           const int k = q / QUADS;
           const int r = (q - k * QUADS) * 4 + r_off;
           if (r < SIMH) {
-            const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
             float s[4 * NQ4];
+            if constexpr (HT) {
+              // odd row pitch: word loads of the 4 + 2 PHM values
+              const float* row = sSim + (k * SIMH + r) * SIMP + 4 * seg;
 #pragma unroll
-            for (int q4 = 0; q4 < NQ4; ++q4) {
-              const float4 v = row[q4];
-              s[4 * q4] = v.x;
-              s[4 * q4 + 1] = v.y;
-              s[4 * q4 + 2] = v.z;
-              s[4 * q4 + 3] = v.w;
+              for (int q = 0; q < 4 + 2 * PHM; ++q) s[q] = row[q];
+            } else {
+              const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
+#pragma unroll
+              for (int q4 = 0; q4 < NQ4; ++q4) {
+                const float4 v = row[q4];
+                s[4 * q4] = v.x;
+                s[4 * q4 + 1] = v.y;
+                s[4 * q4 + 2] = v.z;
+                s[4 * q4 + 3] = v.w;
+              }
             }
             float hs[NP][4];
 #pragma unroll
@@ -614,9 +642,7 @@ template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int 
 __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
   using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
-  // phase A in column triples wherever a batch holds three offsets of InSAR
-  // input (the 8-plane instantiations are at their register limit)
-  constexpr bool HT = L::K == 3 && !L::FULL8;
+  constexpr bool HT = L::HT;
   constexpr int RS = L::RS, RSH = L::RSH, RO = L::RO, TW = L::TW, PX = L::PX;
   constexpr int NT = L::THREADS, NM = L::NM;
   constexpr bool FULL8 = L::FULL8;
