@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kBoxThreads)
                 "window vectors stay inside a staged row");
   static_assert((kBoxTH / 4) * (kBoxTW / 2) == kBoxThreads, "one vertical item per thread");
   extern __shared__ __align__(16) float sm[];
-  float* sI = sm;                                              // [SH][SWP]
+  float* sI = sm;                                              // [SH][SWP]: 2 I = a1^2 + a2^2
   float2* sZ = reinterpret_cast<float2*>(sm + SH * SWP);        // [SH][SWP] (Re, Im)
   float* hI = sm + 3 * SH * SWP;                               // [SH][kBoxTW] horizontal sums
   float2* hZ = reinterpret_cast<float2*>(hI + SH * kBoxTW);     // [SH][kBoxTW]
@@ -243,7 +243,9 @@ __global__ void __launch_bounds__(kBoxThreads)
         float sn, cs;
         __sincosf(ph[u], &sn, &cs);
         const float aa = am[u] * as[u];
-        sI[si] = (am[u] * am[u] + as[u] * as[u]) / 2;
+        // twice the intensity (I1 + I2): the halving is folded into the
+        // output stage (exact: a power of two)
+        sI[si] = am[u] * am[u] + as[u] * as[u];
         sZ[si] = make_float2(aa * cs, aa * sn);
       }
     }
@@ -307,7 +309,8 @@ __global__ void __launch_bounds__(kBoxThreads)
   }
   // outputs on the virtual plane: row H-1 holds virtual row H-1+R (likewise
   // column W-1); a column pair wholly left of column W-1 maps to itself
-  const float inv_n = 1.0f / (float)((2 * R + 1) * (2 * R + 1));
+  // the staged plane holds 2 I: ref = (2 I sum) / (2 n), coh = 2 |sum| / (2 I sum)
+  const float inv_2n = 0.5f / (float)((2 * R + 1) * (2 * R + 1));
   const int vx = vx0 + c0;
   const bool cols_plain = vx + 1 < W - 1;
 #pragma unroll
@@ -320,13 +323,13 @@ __global__ void __launch_bounds__(kBoxThreads)
     for (int e = 0; e < 2; ++e) {
       const float si = e == 0 ? sIp[q].x : sIp[q].y;
       const float sr = sZc[e][q].x, sj = sZc[e][q].y;
-      o_r[e] = si * inv_n;
+      o_r[e] = si * inv_2n;
       o_p[e] = atan2_fast(sj, sr);
       // |sum| / sum I with the hardware square root and the fast division
       // (a few ulps, against the 1e-4 relative tolerance of the coherence)
       float m;
       asm("sqrt.approx.f32 %0, %1;" : "=f"(m) : "f"(sr * sr + sj * sj));
-      o_c[e] = __fdividef(m, si);
+      o_c[e] = __fdividef(2.0f * m, si);
     }
     const size_t rowo = (size_t)oy * W;
     if (cols_plain && vec_out) {

@@ -10,11 +10,11 @@
 // time (seven when every pass has one patch size of at most 7) along a row of
 // the window (same dy, consecutive dx), in the reference's summation order
 // (row-major over the window, compute_nl_statistics.cl:77-78):
-//   A  GLR similarities of the batch on the tile plus the patch halo (three
-//      offsets: each thread three adjacent columns of one row, the neighbour
-//      of column j at offset k being neighbour column j + k, so five
-//      neighbour loads serve nine pairs; seven offsets: each thread one pixel
-//      x the seven offsets); the measure is evaluated in
+//   A  GLR similarities of the batch on the tile plus the patch halo (InSAR
+//      input: each thread three adjacent columns of one row, the neighbour of
+//      column j at offset k being neighbour column j + k, so K + 2 neighbour
+//      loads serve 3 K pairs; 8-plane input: each thread one pixel x the
+//      offsets); the measure is evaluated in
 //      an order symmetric in its two pixels, so the mirrored half window gets
 //      exactly the values of the reference's copy
 //      (center first in the upper half, neighbour first in the mirrored half,
@@ -63,9 +63,8 @@ struct FastL {
   static constexpr int K = (NPX == 1 && PHX <= 3) ? 7 : 3;
   static constexpr int NA = FULL8 ? 12 : 8;          // accumulators per (pixel, patch size)
   static constexpr int NM = FULL8 ? 8 : 4;           // weighted sums kept for the selected combination
-  // phase A in column triples, one row per lane, where a batch holds three
-  // offsets of InSAR input (fast_pass)
-  static constexpr bool HT = K == 3 && !FULL8;
+  // phase A in column triples, one row per lane, for InSAR input (fast_pass)
+  static constexpr bool HT = !FULL8;
   // scaled covariance region: RS x RSH, with one unused pixel more per row
   // for InSAR input, which makes the row pitch odd (fast_stage)
   static constexpr int RS = TW + 2 * (PHX + WSH) + (FULL8 ? 0 : 1);
@@ -291,7 +290,7 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
   constexpr int SIMW = TW + 2 * PHM, SIMH = L::TH + 2 * PHM;  // this pass's similarity region
   constexpr int SIMP = HT ? SIMW + 1 : (SIMW + 7) / 8 * 8;  // row pitch (FastL::SIMPX)
   constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
-  static_assert(HT == L::HT && (!HT || K == 3), "column triples serve three offsets");
+  static_assert(HT == L::HT, "phase A layout");
   static_assert(PH0 >= 0 && NP <= L::NPX && CO >= 0, "pass shape");
   static_assert(SIMP <= L::SIMPX && (HT ? SIMP % 2 == 1 : SIMP >= 4 * 7 + 4 * NQ4),
                 "phase-B segments must stay inside a row");
@@ -357,9 +356,9 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
     for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
       if constexpr (HT) {
         // ---- A, column triples: a thread takes three adjacent columns of
-        // one row of the similarity region for the three offsets; the
-        // neighbour of column j at offset k is neighbour column j + k, so
-        // three centre and five neighbour loads serve the nine pairs.
+        // one row of the similarity region for the K offsets; the neighbour
+        // of column j at offset k is neighbour column j + k, so three centre
+        // and K + 2 neighbour loads serve the 3 K pairs.
         // Consecutive lanes take consecutive rows of one triple of columns:
         // the staged rows (RS float4) and the similarity rows (SIMP words)
         // have odd pitches, so their 16-byte loads (8 lanes at a time) and
@@ -396,7 +395,8 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
           }
         }
       } else {
-        // ---- A: similarities of offsets (dy, dx0..dx0+K-1); one pixel per
+        // ---- A (8-plane input, whose instantiations are at their register
+        // limit): similarities of offsets (dy, dx0..dx0+K-1); one pixel per
         // thread and consecutive pixels on consecutive lanes (conflict free)
         // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
         for (int it = tid; it < SIMH * SIMP; it += NT) {
