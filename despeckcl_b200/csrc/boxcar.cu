@@ -25,8 +25,8 @@ namespace dcl {
 namespace {
 
 constexpr int kBoxTW = 64;
-constexpr int kBoxTH = 32;
-constexpr int kBoxThreads = 256;
+constexpr int kBoxTH = 32;  // 40- and 48-row tiles (2 CTAs per SM) measured slower
+constexpr int kBoxThreads = kBoxTH * 8;  // one vertical item (4 rows x 2 columns) per thread
 constexpr int kBoxMaxR = 15;
 
 __device__ __forceinline__ int clampi_b(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
