@@ -82,10 +82,23 @@ __host__ __device__ constexpr int rev5(int i) {
   return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
 }
 
+// a - b on both lanes of a float pair in one packed (f32x2) instruction,
+// each lane rounded like the scalar subtraction
+__device__ __forceinline__ float2 fsub2_rn(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<const unsigned long long*>(&a)), "l"(*reinterpret_cast<const unsigned long long*>(&b)));
+  return *reinterpret_cast<const float2*>(&r);
+}
+
 // In-register 32-point radix-2 decimation-in-time FFT (forward: e^{-i}, no
 // scaling; inverse: e^{+i}, no scaling).  Every product and sum below is an
 // explicitly rounded intrinsic, so the two Goldstein paths of this file, which
 // share these functions, give the same bits whatever the compiler contracts.
+// The butterflies' complex additions are packed (f32x2) adds and subtractions,
+// rounded per lane exactly like the scalar ones; the twiddle products stay
+// scalar (their factors are constant operands).
 template <bool INV>
 __device__ __forceinline__ void fft32(float2 (&x)[kP]) {
 #pragma unroll
@@ -116,8 +129,14 @@ __device__ __forceinline__ void fft32(float2 (&x)[kP]) {
           const float wy = INV ? -w.y : w.y;
           t = make_float2(__fmaf_rn(b.x, w.x, -__fmul_rn(b.y, wy)), __fmaf_rn(b.x, wy, __fmul_rn(b.y, w.x)));
         }
-        x[i + k] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
-        x[i + k + half] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
+        if (m == 8) {
+          // the pair (+-b.y, -+b.x) would need moves: scalar adds
+          x[i + k] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
+          x[i + k + half] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
+        } else {
+          x[i + k] = __fadd2_rn(a, t);
+          x[i + k + half] = fsub2_rn(a, t);
+        }
       }
     }
   }
@@ -244,9 +263,12 @@ __device__ __forceinline__ void add_sample(float2& v, float fx, float fy, float2
   v.y = __fmaf_rn(f, q.y, v.y);
 }
 
-// |Z| and arg Z (slc2real.cl); the angle within 6e-7 rad (atan2_fast)
+// |Z| and arg Z (slc2real.cl): the magnitude by the hardware square root
+// (a few parts in 1e7), the angle within 6e-7 rad (atan2_fast)
 __device__ __forceinline__ void write_polar(float* __restrict__ ref, float* __restrict__ phase, size_t o, float2 v) {
-  ref[o] = fabsf(sqrtf(__fmaf_rn(v.x, v.x, __fmul_rn(v.y, v.y))));
+  float m;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(m) : "f"(__fmaf_rn(v.x, v.x, __fmul_rn(v.y, v.y))));
+  ref[o] = m;
   phase[o] = atan2_fast(v.y, v.x);
 }
 

@@ -152,16 +152,16 @@ constexpr int kFastTileHHalf = 16;
 
 // Staged regions of the specialised kernel's tile (32 x tile_h outputs), in
 // pixels (width x height): scaled covariance RS x RSH, original covariance
-// RO x ROH.  For InSAR input the scaled covariance box is one pixel wider than
-// the tile and its halo, so that its rows in shared memory have an odd pitch
-// (the kernel's phase A reads it down columns, one row per lane, free of bank
+// RO x ROH.  The scaled covariance box is one pixel wider than the tile and
+// its halo, so that its rows in shared memory have an odd pitch (the
+// kernel's phase A reads it down columns, one row per lane, free of bank
 // conflicts only at an odd pitch); the extra pixel is not used.
 struct FastStage {
   int RS, RSH, RO, ROH;
 };
-__host__ __device__ inline FastStage fast_stage(int wsh, int phm, int tile_h, bool full8) {
+__host__ __device__ inline FastStage fast_stage(int wsh, int phm, int tile_h) {
   FastStage f;
-  f.RS = 32 + 2 * (phm + wsh) + (full8 ? 0 : 1);
+  f.RS = 32 + 2 * (phm + wsh) + 1;
   f.RSH = tile_h + 2 * (phm + wsh);
   f.RO = 32 + 2 * wsh;
   f.ROH = tile_h + 2 * wsh;

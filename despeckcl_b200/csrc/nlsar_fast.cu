@@ -10,11 +10,10 @@
 // time (seven when every pass has one patch size of at most 7) along a row of
 // the window (same dy, consecutive dx), in the reference's summation order
 // (row-major over the window, compute_nl_statistics.cl:77-78):
-//   A  GLR similarities of the batch on the tile plus the patch halo (InSAR
-//      input: each thread three adjacent columns of one row, the neighbour of
-//      column j at offset k being neighbour column j + k, so K + 2 neighbour
-//      loads serve 3 K pairs; 8-plane input: each thread one pixel x the
-//      offsets); the measure is evaluated in
+//   A  GLR similarities of the batch on the tile plus the patch halo (each
+//      thread three adjacent columns of one row, the neighbour of column j at
+//      offset k being neighbour column j + k, so K + 2 neighbour loads serve
+//      3 K pairs); the measure is evaluated in
 //      an order symmetric in its two pixels, so the mirrored half window gets
 //      exactly the values of the reference's copy
 //      (center first in the upper half, neighbour first in the mirrored half,
@@ -63,22 +62,17 @@ struct FastL {
   static constexpr int K = (NPX == 1 && PHX <= 3) ? 7 : 3;
   static constexpr int NA = FULL8 ? 12 : 8;          // accumulators per (pixel, patch size)
   static constexpr int NM = FULL8 ? 8 : 4;           // weighted sums kept for the selected combination
-  // phase A in column triples, one row per lane, for InSAR input (fast_pass)
-  static constexpr bool HT = !FULL8;
-  // scaled covariance region: RS x RSH, with one unused pixel more per row
-  // for InSAR input, which makes the row pitch odd (fast_stage)
-  static constexpr int RS = TW + 2 * (PHX + WSH) + (FULL8 ? 0 : 1);
+  // scaled covariance region: RS x RSH, with one unused pixel more per row,
+  // which makes the row pitch odd (phase A reads it down columns; fast_stage)
+  static constexpr int RS = TW + 2 * (PHX + WSH) + 1;
   static constexpr int RSH = TH + 2 * (PHX + WSH);
   static constexpr int RO = TW + 2 * WSH;            // original covariance region: RO x ROH
   static constexpr int ROH = TH + 2 * WSH;
-  // similarity region of the widest pass, SIMWX x SIMHX.  Row pitch: odd
-  // with column triples (phase A's lanes write down a column; phase B's
-  // quarter warps, one row each, then read words of four rows that fall in
-  // different banks), else a multiple of 8 words (phase A's lanes write
-  // consecutive words, phase B reads 16-byte vectors, a quarter warp covering
-  // 8 consecutive segments of one row: contiguous, conflict free)
+  // similarity region of the widest pass, SIMWX x SIMHX, at an odd row pitch
+  // (phase A's lanes write down a column; phase B's quarter warps, one row
+  // each, then read words of four rows that fall in different banks)
   static constexpr int SIMWX = TW + 2 * PHX, SIMHX = TH + 2 * PHX;
-  static constexpr int SIMPX = HT ? SIMWX + 1 : (SIMWX + 7) / 8 * 8;
+  static constexpr int SIMPX = SIMWX + 1;
   static constexpr int HP = TW;                      // horizontal-sum row pitch (words), unpadded
   static constexpr int HPL = K * SIMHX * HP;         // one patch size's horizontal-sum plane
   // shared memory, in 4-byte words; the TMA destinations start on 128-byte
@@ -278,7 +272,7 @@ struct Best {
 // combinations update the selection state.  The staged scaled covariance
 // carries the halo of the call's largest patch; a pass with smaller patches
 // reads its region CO pixels further in.
-template <class L, int PH0, int PH1, int PH2, int PV, bool HT>
+template <class L, int PH0, int PH1, int PH2, int PV>
 __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParams& pp, float* smem,
                                           Best<L::PX, L::NM>& best) {
   constexpr int WSH = L::WSH, K = L::K, RS = L::RS, RO = L::RO, TW = L::TW, PX = L::PX;
@@ -288,11 +282,9 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
   constexpr int PHM = cmax(PH0, cmax(PH1, PH2));
   constexpr int CO = L::PHX - PHM;
   constexpr int SIMW = TW + 2 * PHM, SIMH = L::TH + 2 * PHM;  // this pass's similarity region
-  constexpr int SIMP = HT ? SIMW + 1 : (SIMW + 7) / 8 * 8;  // row pitch (FastL::SIMPX)
-  constexpr int NQ4 = (4 + 2 * PHM + 3) / 4;  // 16-byte loads per phase-B row segment
-  static_assert(HT == L::HT, "phase A layout");
+  constexpr int SIMP = SIMW + 1;  // odd row pitch (FastL::SIMPX)
   static_assert(PH0 >= 0 && NP <= L::NPX && CO >= 0, "pass shape");
-  static_assert(SIMP <= L::SIMPX && (HT ? SIMP % 2 == 1 : SIMP >= 4 * 7 + 4 * NQ4),
+  static_assert(SIMP <= L::SIMPX && SIMP % 2 == 1 && 4 * 7 + 4 + 2 * PHM <= SIMW,
                 "phase-B segments must stay inside a row");
   const float4* sCs = reinterpret_cast<const float4*>(smem + L::OFF_CS);
   const float4* sCo = reinterpret_cast<const float4*>(smem + L::OFF_CO);
@@ -354,7 +346,7 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
 
   for (int dy = -WSH; dy <= WSH; ++dy) {
     for (int dx0 = -WSH; dx0 <= WSH; dx0 += K) {
-      if constexpr (HT) {
+      {
         // ---- A, column triples: a thread takes three adjacent columns of
         // one row of the similarity region for the K offsets; the neighbour
         // of column j at offset k is neighbour column j + k, so three centre
@@ -394,22 +386,6 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
             for (int k = 0; k < K; ++k) out[k * SIMH * SIMP + j] = glr_sim<PV>(a, la, b[j + k], lb[j + k], c2d);
           }
         }
-      } else {
-        // ---- A (8-plane input, whose instantiations are at their register
-        // limit): similarities of offsets (dy, dx0..dx0+K-1); one pixel per
-        // thread and consecutive pixels on consecutive lanes (conflict free)
-        // rows padded to a multiple of 8 lanes so no quarter warp straddles a row
-        for (int it = tid; it < SIMH * SIMP; it += NT) {
-          const int r = it / SIMP;
-          const int c = it - r * SIMP;
-          if (c >= SIMW) continue;
-          const int ci = (r + WSH + CO) * RS + (c + WSH + CO);
-          const float4 a = sCs[ci];
-          const float la = sLd[ci];
-          const int ni = ci + dy * RS + dx0;
-#pragma unroll
-          for (int k = 0; k < K; ++k) sSim[k * SIMH * SIMP + it] = glr_sim<PV>(a, la, sCs[ni + k], sLd[ni + k], c2d);
-        }
       }
       __syncthreads();
       // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
@@ -423,23 +399,11 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
           const int k = q / QUADS;
           const int r = (q - k * QUADS) * 4 + r_off;
           if (r < SIMH) {
-            float s[4 * NQ4];
-            if constexpr (HT) {
-              // odd row pitch: word loads of the 4 + 2 PHM values
-              const float* row = sSim + (k * SIMH + r) * SIMP + 4 * seg;
+            // odd row pitch: word loads of the 4 + 2 PHM values
+            float s[4 + 2 * PHM];
+            const float* row = sSim + (k * SIMH + r) * SIMP + 4 * seg;
 #pragma unroll
-              for (int q = 0; q < 4 + 2 * PHM; ++q) s[q] = row[q];
-            } else {
-              const float4* row = reinterpret_cast<const float4*>(sSim + (k * SIMH + r) * SIMP + 4 * seg);
-#pragma unroll
-              for (int q4 = 0; q4 < NQ4; ++q4) {
-                const float4 v = row[q4];
-                s[4 * q4] = v.x;
-                s[4 * q4 + 1] = v.y;
-                s[4 * q4 + 2] = v.z;
-                s[4 * q4 + 3] = v.w;
-              }
-            }
+            for (int q = 0; q < 4 + 2 * PHM; ++q) s[q] = row[q];
             float hs[NP][4];
 #pragma unroll
             for (int o = 0; o < 4; ++o) {
@@ -642,7 +606,6 @@ template <int WSH, int PHX, int A0, int A1, int A2, int B0, int B1, int B2, int 
 __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L::THREADS, 1)
     nlsar_fast_kernel(const FilterParams P, const SceneDesc* __restrict__ scenes) {
   using L = typename FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, TH_, FULL8_>::L;
-  constexpr bool HT = L::HT;
   constexpr int RS = L::RS, RSH = L::RSH, RO = L::RO, TW = L::TW, PX = L::PX;
   constexpr int NT = L::THREADS, NM = L::NM;
   constexpr bool FULL8 = L::FULL8;
@@ -718,12 +681,12 @@ __global__ void __launch_bounds__(FastK<WSH, PHX, A0, A1, A2, B0, B1, B2, PX_, T
         loaded_slot = pp.scale_slot;
       }
       if constexpr (B0 < 0) {
-        fast_pass<L, A0, A1, A2, PV, HT>(P, pp, smem, best);
+        fast_pass<L, A0, A1, A2, PV>(P, pp, smem, best);
       } else {
         if (pass_is<A0, A1, A2>(pp))
-          fast_pass<L, A0, A1, A2, PV, HT>(P, pp, smem, best);
+          fast_pass<L, A0, A1, A2, PV>(P, pp, smem, best);
         else
-          fast_pass<L, B0, B1, B2, PV, HT>(P, pp, smem, best);
+          fast_pass<L, B0, B1, B2, PV>(P, pp, smem, best);
       }
     }
 

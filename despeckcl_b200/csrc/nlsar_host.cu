@@ -391,7 +391,7 @@ int carve_scene(const Plan& pl, const SceneGeom& g, char* base, SceneDesc& d) {
   // (vx0 - wsh + G, vy0 - wsh + G) and the scaled covariance box at
   // (vx0 - phm - wsh + G, vy0 - phm - wsh + G), in float4 pixels: x origins
   // in floats are multiples of 4 (16 bytes), as the TMA unit requires
-  const FastStage fs = fast_stage(pl.P.wsh, pl.P.phm, pl.P.tile_h, pl.full8);
+  const FastStage fs = fast_stage(pl.P.wsh, pl.P.phm, pl.P.tile_h);
   const uint64_t Hp = (uint64_t)g.Hp, pitch = (uint64_t)g.pitch;
   int rc = encode_map_2d(&d.tm_co, d.cori, 4 * pitch, Hp, pitch * 16, 4 * fs.RO, fs.ROH);
   if (rc == DCL_OK && pl.full8) rc = encode_map_2d(&d.tm_co2, d.cori2, 4 * pitch, Hp, pitch * 16, 4 * fs.RO, fs.ROH);
