@@ -389,8 +389,9 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
       }
       __syncthreads();
       // ---- B: horizontal sums, 4 output columns per item.  A warp takes a
-      // quad of rows x 8 column segments, each quarter warp one row, so its
-      // 16-byte loads and stores are contiguous.
+      // quad of rows x 8 column segments, each quarter warp one row: word
+      // loads (the odd similarity pitch puts the four rows in different
+      // banks) and contiguous 16-byte stores.
       {
         constexpr int QUADS = (SIMH + 3) / 4;
         const int r_off = lane >> 3;
@@ -403,7 +404,7 @@ __device__ __forceinline__ void fast_pass(const FilterParams& P, const PassParam
             float s[4 + 2 * PHM];
             const float* row = sSim + (k * SIMH + r) * SIMP + 4 * seg;
 #pragma unroll
-            for (int q = 0; q < 4 + 2 * PHM; ++q) s[q] = row[q];
+            for (int e = 0; e < 4 + 2 * PHM; ++e) s[e] = row[e];
             float hs[NP][4];
 #pragma unroll
             for (int o = 0; o < 4; ++o) {
