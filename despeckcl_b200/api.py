@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
         L.dcl_stats_collection_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StatsEntry)]
         L.dcl_stats_collection_free.argtypes = [ctypes.c_void_p]
         L.dcl_stats_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.dcl_stats_save_boost_text.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.dcl_stats_load.argtypes = [ctypes.c_char_p]
         L.dcl_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(StatsEntry),
@@ -209,14 +210,23 @@ def _from_handle(h) -> StatsCollection:
         L.dcl_stats_collection_free(h)
 
 
-def store_nlsar_stats_collection(nsc, filename: str) -> None:
-    """Stores a statistics collection (nlsar.i:29-34)."""
+def store_nlsar_stats_collection(nsc, filename: str, format: str = "boost") -> None:
+    """Stores a statistics collection (nlsar.i:29-34).
+
+    format="boost" writes the reference's file, a Boost text archive of
+    std::map<nlsar::params, nlsar::stats> (nlsar_training.cpp:99-104), which
+    the reference's load_nlsar_stats_collection reads; format="native" writes
+    this library's own versioned text format.  load_nlsar_stats_collection
+    reads both."""
+    if format not in ("boost", "native"):
+        raise ValueError(f"format must be 'boost' or 'native', not {format!r}")
     arr, n, keep = _entries(nsc)
     h = lib().dcl_stats_collection_from_entries(arr, n)
     if not h:
         raise DespeckclError(-1, lib().dcl_last_error().decode(errors="replace"))
     try:
-        _check(lib().dcl_stats_save(h, os.fsencode(filename)))
+        save = lib().dcl_stats_save_boost_text if format == "boost" else lib().dcl_stats_save
+        _check(save(h, os.fsencode(filename)))
     finally:
         lib().dcl_stats_collection_free(h)
 

@@ -194,7 +194,8 @@ nlsar_stats_collection despeckcl::nlsar_training(float* covmat_raw, const int he
 void despeckcl::store_nlsar_stats_collection(nlsar_stats_collection nsc, std::string filename) {
   const std::vector<dcl_stats_entry> e = entries_of(nsc);
   dcl_stats_collection* c = dcl_stats_collection_from_entries(e.data(), (int)e.size());
-  const int rc = c ? dcl_stats_save(c, filename.c_str()) : DCL_ERR_INVALID_ARGUMENT;
+  // the reference's file: a Boost text archive of the map
+  const int rc = c ? dcl_stats_save_boost_text(c, filename.c_str()) : DCL_ERR_INVALID_ARGUMENT;
   dcl_stats_collection_free(c);
   if (rc != DCL_OK) throw std::runtime_error(std::string("store_nlsar_stats_collection: ") + dcl_last_error());
 }

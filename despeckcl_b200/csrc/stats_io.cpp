@@ -197,67 +197,153 @@ extern "C" int dcl_stats_save(const dcl_stats_collection* c, const char* filenam
   return ok ? DCL_OK : dcl::set_error(DCL_ERR_IO, "error writing %s", filename);
 }
 
-// Best-effort reader of a Boost text archive of std::map<nlsar::params,
-// nlsar::stats> (fields serialised at include/compute/nlsar/parameters.h:51-55
-// and stats.h:43-50 of the reference).  Boost inserts class-tracking and
-// version numbers whose exact placement depends on the Boost version; this
-// reader skips them by matching the shape "patch scale L min max L q[L] L c[L]"
-// with an item-version word after each vector length (as modern Boost
-// writes it), or without one.  Unverified against a real archive: Boost is
-// not available to produce one.
-static dcl_stats_collection* load_boost_text(const std::vector<std::string>& tok) {
-  std::vector<double> v;
-  for (size_t i = 0; i < tok.size(); ++i) {
+// Boost text archives of std::map<nlsar::params, nlsar::stats>, the file the
+// reference's store_nlsar_stats_collection writes
+// (src/compute/nlsar/training/nlsar_training.cpp:99-104: a text_oarchive
+// given the whole map).  Boost is not used; the layout follows
+// Boost.Serialization's save rules for these types:
+//
+//   22 serialization::archive V         signature (length, text), format version
+//   t v                                 class info of the map (tracking, version)
+//   N i                                 element count, item version
+//   first element:  t v                 class info of std::pair
+//                   t v p s             class info of params, then
+//                                       patch_size scale_size (parameters.h:51-55)
+//                   t v L dmin dmax     class info of stats, then lut_size,
+//                                       dissims_min, dissims_max (stats.h:43-50)
+//                   L i q[0..L-1]       quantilles: count, item version, values
+//                   L i c[0..L-1]       chi2cdf_inv, the same
+//   later elements: p s L dmin dmax L i q[...] L i c[...]
+//
+// Class info (one tracking word and one class-version word) precedes only
+// the first object of each class type; vectors of a primitive type carry
+// none (Boost gives them the object_serializable level).  Objects that are
+// never saved through a pointer are untracked, so every tracking word is 0
+// and no object ids follow.  Format versions 3 and below have no item-version
+// words; the layout is otherwise the same in every version.
+
+namespace {
+
+// A strict reader over the archive's whitespace-separated tokens.
+struct BoostTokens {
+  const std::vector<std::string>& tok;
+  size_t k;
+  bool ok = true;
+  const char* what = nullptr;
+
+  bool fail(const char* w) {
+    if (ok) what = w;
+    ok = false;
+    return false;
+  }
+  bool next_long(long& out, const char* w) {
+    if (!ok) return false;
+    if (k >= tok.size()) return fail(w);
+    const char* s = tok[k].c_str();
     char* end = nullptr;
-    const double x = std::strtod(tok[i].c_str(), &end);
-    if (end && *end == '\0') v.push_back(x);
+    out = std::strtol(s, &end, 10);
+    if (end == s || *end != '\0') return fail(w);
+    ++k;
+    return true;
   }
+  bool next_float(float& out, const char* w) {
+    if (!ok) return false;
+    if (k >= tok.size()) return fail(w);
+    const char* s = tok[k].c_str();
+    char* end = nullptr;
+    out = std::strtof(s, &end);
+    if (end == s || *end != '\0') return fail(w);
+    ++k;
+    return true;
+  }
+  // tracking and class-version words of a class's first object
+  bool class_info(const char* w) {
+    long tracking = -1, version = -1;
+    if (!next_long(tracking, w) || !next_long(version, w)) return false;
+    if (tracking != 0) return fail("tracked objects (not written by a map of NL-SAR statistics)");
+    if (version < 0) return fail(w);
+    return true;
+  }
+  bool vec(std::vector<float>& v, long library_version, const char* w) {
+    long n = -1, item_version = 0;
+    if (!next_long(n, w)) return false;
+    if (n < 0 || n > (1L << 24)) return fail(w);
+    if (library_version > 3 && !next_long(item_version, w)) return false;
+    v.resize((size_t)n);
+    for (long i = 0; i < n && ok; ++i) next_float(v[(size_t)i], w);
+    return ok;
+  }
+};
+
+}  // namespace
+
+static dcl_stats_collection* load_boost_text(const std::vector<std::string>& tok, const char* filename) {
+  BoostTokens in{tok, 2};
+  long version = -1, n = -1, item_version = 0;
+  in.next_long(version, "archive format version");
+  if (in.ok && version < 1) in.fail("archive format version");
+  in.class_info("class info of the map");
+  in.next_long(n, "element count");
+  if (in.ok && n < 0) in.fail("element count");
+  if (version > 3) in.next_long(item_version, "item version");
   dcl_stats_collection* c = new dcl_stats_collection();
-  size_t i = 0;
-  auto is_int = [](double x) { return std::floor(x) == x; };
-  while (i + 6 < v.size()) {
-    bool matched = false;
-    const double p = v[i], s = v[i + 1];
-    if (is_int(p) && is_int(s) && p >= 1 && s >= 1 && ((long)p % 2) && ((long)s % 2)) {
-      // up to two class-tracking / version words may sit between the key and
-      // the stats fields, and one item-version word after each vector length
-      for (int skip = 0; skip <= 2 && !matched; ++skip) {
-        const size_t l0 = i + 2 + skip;
-        if (l0 + 3 >= v.size()) break;
-        bool small_ints = true;
-        for (int k = 0; k < skip; ++k) small_ints = small_ints && is_int(v[i + 2 + k]) && v[i + 2 + k] >= 0 && v[i + 2 + k] <= 1;
-        const double L = v[l0];
-        if (!small_ints || !is_int(L) || L < 2 || L > 4096) continue;
-        for (int iv1 = 1; iv1 >= 0 && !matched; --iv1) {
-          size_t q0 = l0 + 3;
-          if (q0 >= v.size() || v[q0] != L) continue;
-          q0 += 1 + iv1;
-          const size_t c0 = q0 + (size_t)L;
-          for (int iv2 = 1; iv2 >= 0 && !matched; --iv2) {
-            if (c0 >= v.size() || v[c0] != L) continue;
-            const size_t cc = c0 + 1 + iv2;
-            if (cc + (size_t)L > v.size()) continue;
-            OwnedStats st;
-            st.lut_size = (unsigned)L;
-            st.dmin = (float)v[l0 + 1];
-            st.dmax = (float)v[l0 + 2];
-            for (size_t k = 0; k < (size_t)L; ++k) st.quant.push_back((float)v[q0 + k]);
-            for (size_t k = 0; k < (size_t)L; ++k) st.chi2.push_back((float)v[cc + k]);
-            c->entries[{(int)p, (int)s}] = std::move(st);
-            i = cc + (size_t)L;
-            matched = true;
-          }
-        }
-      }
+  for (long e = 0; e < n && in.ok; ++e) {
+    if (e == 0) {
+      in.class_info("class info of the (params, stats) pair");
+      in.class_info("class info of params");
     }
-    if (!matched) ++i;
+    long p = 0, s = 0, L = 0;
+    in.next_long(p, "patch_size");
+    in.next_long(s, "scale_size");
+    if (e == 0) in.class_info("class info of stats");
+    in.next_long(L, "lut_size");
+    OwnedStats st;
+    in.next_float(st.dmin, "dissims_min");
+    in.next_float(st.dmax, "dissims_max");
+    in.vec(st.quant, version, "quantilles");
+    in.vec(st.chi2, version, "chi2cdf_inv");
+    if (!in.ok) break;
+    if (L < 0 || (size_t)L != st.quant.size() || (size_t)L != st.chi2.size()) {
+      in.fail("lut_size against the table lengths");
+      break;
+    }
+    st.lut_size = (unsigned)L;
+    c->entries[{(int)p, (int)s}] = std::move(st);
   }
-  if (c->entries.empty()) {
+  if (in.ok && in.k != tok.size()) in.fail("trailing words after the last element");
+  if (!in.ok) {
     delete c;
-    dcl::set_error(DCL_ERR_IO, "no NL-SAR statistics found in the archive");
+    dcl::set_error(DCL_ERR_IO, "%s: Boost text archive: bad or missing %s (word %zu)", filename, in.what, in.k);
     return nullptr;
   }
   return c;
+}
+
+extern "C" int dcl_stats_save_boost_text(const dcl_stats_collection* c, const char* filename) {
+  if (!c || !filename) return dcl::set_error(DCL_ERR_INVALID_ARGUMENT, "null collection or filename");
+  FILE* f = std::fopen(filename, "w");
+  if (!f) return dcl::set_error(DCL_ERR_IO, "cannot open %s for writing", filename);
+  // format version 10: Boost reads every version up to its own, and these
+  // types are laid out the same from version 4 on
+  std::fprintf(f, "22 serialization::archive 10 0 0 %zu 0", c->entries.size());
+  bool first = true;
+  for (auto& kv : c->entries) {
+    const OwnedStats& s = kv.second;
+    if (first) std::fprintf(f, " 0 0 0 0");
+    std::fprintf(f, " %d %d", kv.first.first, kv.first.second);
+    if (first) std::fprintf(f, " 0 0");
+    std::fprintf(f, " %u %.9e %.9e", s.lut_size, s.dmin, s.dmax);
+    // floats as Boost's text archive writes them: scientific, 9 digits after
+    // the point (an exact round trip for every float)
+    std::fprintf(f, " %zu 0", s.quant.size());
+    for (float q : s.quant) std::fprintf(f, " %.9e", q);
+    std::fprintf(f, " %zu 0", s.chi2.size());
+    for (float q : s.chi2) std::fprintf(f, " %.9e", q);
+    first = false;
+  }
+  std::fprintf(f, "\n");
+  const bool ok = std::fclose(f) == 0;
+  return ok ? DCL_OK : dcl::set_error(DCL_ERR_IO, "error writing %s", filename);
 }
 
 extern "C" dcl_stats_collection* dcl_stats_load(const char* filename) {
@@ -299,7 +385,7 @@ extern "C" dcl_stats_collection* dcl_stats_load(const char* filename) {
     }
     return c;
   }
-  if (tok.size() >= 2 && tok[1] == "serialization::archive") return load_boost_text(tok);
+  if (tok.size() >= 2 && tok[0] == "22" && tok[1] == "serialization::archive") return load_boost_text(tok, filename);
   dcl::set_error(DCL_ERR_IO, "%s: not an NL-SAR statistics file", filename);
   return nullptr;
 }

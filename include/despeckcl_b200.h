@@ -14,7 +14,7 @@
  *                                                                          src/compute/nlsar/nlsar.cpp:171-194
  *   dcl_nlsar_training_*     despeckcl::nlsar_training(...)              include/despeckcl.h:75-92,
  *                                                                          src/compute/nlsar/training/nlsar_training.cpp:57-96
- *   dcl_stats_save/load      despeckcl::store/load_nlsar_stats_collection include/despeckcl.h:94-95,
+ *   dcl_stats_save, _load    despeckcl::store/load_nlsar_stats_collection include/despeckcl.h:94-95,
  *                                                                          src/compute/nlsar/training/nlsar_training.cpp:99-113
  *   dcl_boxcar*              despeckcl::boxcar(...)                      include/despeckcl.h:34-43,
  *                                                                          src/compute/boxcar/boxcar.cpp:30-100
@@ -318,10 +318,17 @@ dcl_stats_collection* dcl_stats_collection_from_entries(const dcl_stats_entry* e
 void dcl_stats_collection_free(dcl_stats_collection* c);
 
 /* Store / load a statistics collection (despeckcl::store/load_nlsar_stats_collection,
- * include/despeckcl.h:94-95).  The file is this library's versioned text format;
- * dcl_stats_load also reads Boost text archives of std::map<nlsar::params,
- * nlsar::stats> as written by the reference. */
+ * include/despeckcl.h:94-95).
+ * dcl_stats_save writes this library's versioned text format.
+ * dcl_stats_save_boost_text writes the file the reference's
+ * store_nlsar_stats_collection writes (src/compute/nlsar/training/nlsar_training.cpp:99-104):
+ * a Boost text archive of std::map<nlsar::params, nlsar::stats>, produced
+ * without Boost; the reference's load_nlsar_stats_collection reads it.
+ * dcl_stats_load reads either, telling them apart by their first words; a
+ * Boost archive is parsed strictly (class-info, count and item-version words
+ * where Boost writes them) and a malformed one fails with DCL_ERR_IO. */
 int dcl_stats_save(const dcl_stats_collection* c, const char* filename);
+int dcl_stats_save_boost_text(const dcl_stats_collection* c, const char* filename);
 dcl_stats_collection* dcl_stats_load(const char* filename);
 
 #ifdef __cplusplus

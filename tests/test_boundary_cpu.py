@@ -106,37 +106,92 @@ def test_chi2_table_matches_scipy():
     assert st.chi2cdf_inv[255] == 100000
 
 
-def test_stats_file_round_trip(tmp_path, train_stats):
+# tests/golden/nlsar_stats_boost.txt: the Boost text archive that the
+# reference's store_nlsar_stats_collection (nlsar_training.cpp:99-104) writes
+# for a map of two entries, laid out word by word from Boost.Serialization's
+# save rules (not produced by Boost, which is absent here):
+#   "22 serialization::archive 10"   signature and format version
+#   "0 0"                            map: tracking 0, class version 0
+#   "2 0"                            two elements, item version 0
+#   "0 0" "0 0" "3 1"                pair and params class info, key (3, 1)
+#   "0 0" "4 1.5 9.25"               stats class info, lut_size, dissims_min/max
+#   "4 0 q0..q3" "4 0 c0..c3"        quantilles and chi2cdf_inv (count, item version)
+#   "5 3 4 2 12 4 0 ... 4 0 ..."     second element: no class info any more
+# Floats appear as Boost prints them (scientific, 9 digits after the point).
+BOOST_GOLDEN = os.path.join(ROOT, "tests", "golden", "nlsar_stats_boost.txt")
+BOOST_GOLDEN_STATS = {
+    (3, 1): (4, 1.5, 9.25, [0, 0.25, 0.5, 1], [0, 30.5, 45, 100000]),
+    (5, 3): (4, 2.0, 12.0, [0, 0.5, 0.75, 1], [0, 30.5, 45, 100000]),
+}
+
+
+def _golden_collection():
+    return {k: dcl.Stats(L, lo, hi, np.array(q, np.float32), np.array(c, np.float32))
+            for k, (L, lo, hi, q, c) in BOOST_GOLDEN_STATS.items()}
+
+
+def _check_golden_values(back):
+    assert list(back.keys()) == sorted(BOOST_GOLDEN_STATS)
+    for k, (L, lo, hi, q, c) in BOOST_GOLDEN_STATS.items():
+        assert (back[k].lut_size, back[k].dissims_min, back[k].dissims_max) == (L, lo, hi)
+        np.testing.assert_array_equal(back[k].quantilles, q)
+        np.testing.assert_array_equal(back[k].chi2cdf_inv, c)
+
+
+def test_boost_text_archive_golden_read():
+    _check_golden_values(dcl.load_nlsar_stats_collection(BOOST_GOLDEN))
+
+
+def test_boost_text_archive_writer_matches_golden(tmp_path):
+    f = tmp_path / "stats.txt"
+    dcl.store_nlsar_stats_collection(_golden_collection(), str(f))
+    assert f.read_text() == open(BOOST_GOLDEN).read()
+
+
+def test_boost_text_archive_other_writers(tmp_path):
+    # the same map as an older Boost prints it (default float format, another
+    # format version) and in format version 3 (no item-version words)
+    v17 = ("22 serialization::archive 17 0 0 2 0 0 0 0 0 3 1 0 0 4 1.5 9.25 4 0 0 0.25 0.5 1 4 0 0 30.5 45 100000 "
+           "5 3 4 2 12 4 0 0 0.5 0.75 1 4 0 0 30.5 45 100000")
+    v3 = ("22 serialization::archive 3 0 0 2 0 0 0 0 3 1 0 0 4 1.5 9.25 4 0 0.25 0.5 1 4 0 30.5 45 100000 "
+          "5 3 4 2 12 4 0 0.5 0.75 1 4 0 30.5 45 100000")
+    for text in (v17, v3):
+        f = tmp_path / "a.txt"
+        f.write_text(text + "\n")
+        _check_golden_values(dcl.load_nlsar_stats_collection(str(f)))
+
+
+def test_boost_text_archive_malformed(tmp_path):
+    words = open(BOOST_GOLDEN).read().split()
+    bad = {
+        "truncated": words[:-1],
+        "trailing word": words + ["7"],
+        "tracked map": words[:3] + ["1"] + words[4:],
+        "lut_size against the tables": words[:15] + ["5"] + words[16:],
+        "not a number": words[:20] + ["x"] + words[21:],
+    }
+    for name, w in bad.items():
+        f = tmp_path / "bad.txt"
+        f.write_text(" ".join(w) + "\n")
+        with pytest.raises(dcl.DespeckclError, match="Boost text archive"):
+            dcl.load_nlsar_stats_collection(str(f))
+
+
+def test_stats_file_round_trip_both_formats(tmp_path, train_stats):
     coll = {k: dcl.Stats(v.lut_size, v.dissims_min, v.dissims_max, v.quantilles, v.chi2cdf_inv)
             for k, v in train_stats.items()}
-    f = str(tmp_path / "nlsar_stats.txt")
-    dcl.store_nlsar_stats_collection(coll, f)
-    back = dcl.load_nlsar_stats_collection(f)
-    assert list(back.keys()) == sorted(coll.keys())
-    for k in coll:
-        a, b = coll[k], back[k]
-        assert (a.lut_size, a.dissims_min, a.dissims_max) == (b.lut_size, b.dissims_min, b.dissims_max)
-        np.testing.assert_array_equal(a.quantilles, b.quantilles)
-        np.testing.assert_array_equal(a.chi2cdf_inv, b.chi2cdf_inv)
-
-
-def test_boost_text_archive_reader(tmp_path):
-    # the shape of a Boost text archive of std::map<nlsar::params, nlsar::stats>:
-    # header, map count, item version, class-info words, then the fields of
-    # parameters.h:51-55 and stats.h:43-50 (vector = count, item version, values)
-    L = 4
-    words = ["22", "serialization::archive", "17", "2", "0", "0", "0", "0",
-             "3", "1", "0", "0", str(L), "1.5", "9.25", str(L), "0", "0", "0.25", "0.5", "1",
-             str(L), "0", "0", "30.5", "45", "100000",
-             "5", "3", str(L), "2", "12", str(L), "0", "0", "0.5", "0.75", "1", str(L), "0", "0", "30.5", "45",
-             "100000"]
-    f = tmp_path / "boost.txt"
-    f.write_text(" ".join(words) + "\n")
-    back = dcl.load_nlsar_stats_collection(str(f))
-    assert list(back.keys()) == [(3, 1), (5, 3)]
-    assert back[(3, 1)].dissims_min == 1.5 and back[(3, 1)].dissims_max == 9.25
-    np.testing.assert_array_equal(back[(5, 3)].quantilles, [0, 0.5, 0.75, 1])
-    np.testing.assert_array_equal(back[(3, 1)].chi2cdf_inv, [0, 30.5, 45, 100000])
+    for fmt in ("boost", "native"):
+        f = str(tmp_path / f"stats_{fmt}.txt")
+        dcl.store_nlsar_stats_collection(coll, f, format=fmt)
+        first = open(f).read().split()[:2]
+        assert first == (["22", "serialization::archive"] if fmt == "boost" else ["despeckcl_b200-nlsar-stats", "1"])
+        back = dcl.load_nlsar_stats_collection(f)
+        assert list(back.keys()) == sorted(coll.keys())
+        for k in coll:
+            a, b = coll[k], back[k]
+            assert (a.lut_size, a.dissims_min, a.dissims_max) == (b.lut_size, b.dissims_min, b.dissims_max)
+            np.testing.assert_array_equal(a.quantilles, b.quantilles)
+            np.testing.assert_array_equal(a.chi2cdf_inv, b.chi2cdf_inv)
 
 
 def test_cpp_api_compiles_and_links(tmp_path):
