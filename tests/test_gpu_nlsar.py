@@ -391,6 +391,32 @@ def test_boxcar_matches_oracle(oracle):
         np.testing.assert_allclose(g[2], o[2], rtol=1e-4, atol=1e-6)
 
 
+def test_boxcar_plane_alignment(oracle):
+    # rows a multiple of 4 long, planes at 16-byte boundaries (the host entry
+    # point's buffers) and one float past them (device views into a larger
+    # buffer): same bits, and the oracle's values within tolerance
+    H, W = 300, 528
+    a1, a2, ph = synthetic.insar_scene(H, W, 14)
+    n = H * W
+    flat = torch.empty(3 * n + 4, dtype=torch.float32, device="cuda")
+    for w in (1, 3, 7, 9, 15):
+        o = oracle.boxcar(a1, a2, ph, w)
+        g = dcl.boxcar(a1, a2, ph, w)
+        np.testing.assert_allclose(g[0], o[0], rtol=1e-5)
+        np.testing.assert_array_less(wrapped(g[1] - o[1]), 1e-4)
+        np.testing.assert_allclose(g[2], o[2], rtol=1e-4, atol=1e-6)
+        planes = []
+        for i, a in enumerate((a1, a2, ph)):
+            v = flat[1 + i * n:1 + (i + 1) * n].view(H, W)
+            v.copy_(torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)))
+            assert v.data_ptr() % 16 != 0
+            planes.append(v)
+        d = dcl.boxcar_device(*planes, w)
+        torch.cuda.synchronize()
+        for x, y in zip(g, d):
+            np.testing.assert_array_equal(x, y.cpu().numpy())
+
+
 def test_training_matches_oracle(oracle):
     t1, t2, tp = synthetic.training_area(128, seed=7)
     mine = dcl.nlsar_train_insar(t1, t2, tp, PATCHES, SCALES)
