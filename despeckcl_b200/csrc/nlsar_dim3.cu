@@ -421,7 +421,8 @@ struct Fast3 {
   static constexpr int OFF_SIM = OFF_LD + RN;  // [K][SIMH][SIMP]
   static constexpr int OFF_H = OFF_SIM + K * SIMHX * SIMPX;
   static constexpr int OFF_LUT = OFF_H + NPX * HPL;
-  static constexpr int OFF_X = OFF_LUT + NPX * kMaxLut * LUTREP;  // group 0 -> group 1: take, alpha, s0
+  static constexpr int OFF_W = OFF_LUT + NPX * kMaxLut * LUTREP;  // [K][NPX][32 TH] weights of a batch
+  static constexpr int OFF_X = OFF_W + K * NPX * 32 * TH;          // group 0 -> group 1: take, alpha, s0
   static constexpr int WORDS = OFF_X + 3 * 32 * TH;
   static_assert((2 * WSH + 1) % K == 0, "offset batches must tile a window row");
   static_assert(WORDS * 4 <= 227 * 1024, "shared memory");
@@ -467,6 +468,7 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
   float* sSim = smem + L::OFF_SIM;
   float* sH = smem + L::OFF_H;
   float* sLut = smem + L::OFF_LUT;
+  float* sW = smem + L::OFF_W;
   int* sTake = reinterpret_cast<int*>(smem + L::OFF_X);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp / L::TH, y = warp - grp * L::TH;  // warp-uniform group, output row
@@ -564,11 +566,13 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
         }
       }
       __syncthreads();
-      // ---- C: vertical sums, weights, this group's accumulators
+      // ---- C1: vertical sums and weights, each computed once: group g
+      // takes the offsets k = g, g + 2, ... of the batch for its row and
+      // leaves them in shared memory for both groups
 #pragma unroll
       for (int k = 0; k < K; ++k) {
+        if ((k & 1) != grp) continue;
         const int dx = dx0 + k;
-        float w[NP];
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
           const int ph = ph3_of<PH0, PH1, PH2>(j);
@@ -581,9 +585,19 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
           const float t = __fmaf_rz(u, lm1[j], 8388608.0f);
           const int idx = __float_as_int(t) - 0x4B000000;
           const float lw = lut_j[j][idx * L::LUTREP];
-          w[j] = (d > dmax[j]) ? 0.0f : lw;
-          if (dy == 0 && dx == 0) w[j] = 1.0f;
+          float w = (d > dmax[j]) ? 0.0f : lw;
+          if (dy == 0 && dx == 0) w = 1.0f;
+          sW[(k * NP + j) * (32 * L::TH) + px] = w;
         }
+      }
+      __syncthreads();
+      // ---- C2: this group's accumulators, offsets in order
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int dx = dx0 + k;
+        float w[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) w[j] = sW[(k * NP + j) * (32 * L::TH) + px];
         const size_t nfi = cfi + (ptrdiff_t)dy * S.pitch + dx;
         float v[9];
 #pragma unroll
