@@ -373,8 +373,9 @@ __global__ void __launch_bounds__(kT3Threads, 1) nlsar3_kernel(const FilterParam
 //
 // Same tile (32 x 8 outputs) and the same phases as nlsar3_kernel, with the
 // window and patch sizes fixed at compile time and two threads per output
-// pixel: warps 0-7 (group 0) and 8-15 (group 1) own the same 8 rows.  Both
-// compute the pixel's weights; group 0 keeps sum w, sum w^2, sum w I_d^2 and
+// pixel: warps 0-7 (group 0) and 8-15 (group 1) own the same 8 rows.  The
+// two groups share the weights of each offset batch through shared memory,
+// each computing half of them; group 0 keeps sum w, sum w^2, sum w I_d^2 and
 // the weighted sums of the diagonal and upper-triangle planes (14
 // accumulators per patch size), group 1 those of the other nine planes, so a
 // thread holds at most 42 accumulators and the CTA runs 16 warps.  Group 0
