@@ -161,6 +161,14 @@ def test_boost_text_archive_other_writers(tmp_path):
         _check_golden_values(dcl.load_nlsar_stats_collection(str(f)))
 
 
+def test_boost_text_archive_empty_map(tmp_path):
+    # an empty map: class info of the map, count 0, item version, nothing else
+    f = tmp_path / "empty.txt"
+    dcl.store_nlsar_stats_collection({}, str(f))
+    assert f.read_text() == "22 serialization::archive 10 0 0 0 0\n"
+    assert dict(dcl.load_nlsar_stats_collection(str(f))) == {}
+
+
 def test_boost_text_archive_malformed(tmp_path):
     words = open(BOOST_GOLDEN).read().split()
     bad = {
