@@ -492,11 +492,12 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
     dmax[j] = cp.dmax;
     lut_j[j] = sLut + j * kMaxLut * L::LUTREP + (lane & (L::LUTREP - 1));
   }
-  float acc[NP][NA];
+  static_assert(NA % 2 == 0, "accumulators in pairs");
+  float2 acc[NP][NA / 2];  // accumulator a of patch j: component a % 2 of acc[j][a / 2]
 #pragma unroll
   for (int j = 0; j < NP; ++j)
 #pragma unroll
-    for (int a = 0; a < NA; ++a) acc[j][a] = 0.0f;
+    for (int a = 0; a < NA / 2; ++a) acc[j][a] = make_float2(0.0f, 0.0f);
   __syncthreads();
 
   for (int dy = -WSH; dy <= WSH; ++dy) {
@@ -608,20 +609,32 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
           float i2[3];
 #pragma unroll
           for (int d = 0; d < 3; ++d) i2[d] = v[diag_slot(d)] * v[diag_slot(d)];
+          // accumulators that share the weight, two per packed (f32x2) FMA,
+          // each lane rounded like the scalar FMA; sum w as fma(w, 1, sum),
+          // which equals sum + w
 #pragma unroll
           for (int j = 0; j < NP; ++j) {
-            acc[j][0] += w[j];
-            acc[j][1] = fmaf(w[j], w[j], acc[j][1]);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) acc[j][2 + d] = fmaf(w[j], i2[d], acc[j][2 + d]);
-#pragma unroll
-            for (int q = 0; q < 9; ++q) acc[j][5 + q] = fmaf(w[j], v[q], acc[j][5 + q]);
+            const float2 ww = make_float2(w[j], w[j]);
+            float2* A = acc[j];
+            A[0] = __ffma2_rn(ww, make_float2(1.0f, w[j]), A[0]);  // sum w, sum w^2
+            A[1] = __ffma2_rn(ww, make_float2(i2[0], i2[1]), A[1]);
+            A[2] = __ffma2_rn(ww, make_float2(i2[2], v[0]), A[2]);
+            A[3] = __ffma2_rn(ww, make_float2(v[1], v[2]), A[3]);
+            A[4] = __ffma2_rn(ww, make_float2(v[3], v[4]), A[4]);
+            A[5] = __ffma2_rn(ww, make_float2(v[5], v[6]), A[5]);
+            A[6] = __ffma2_rn(ww, make_float2(v[7], v[8]), A[6]);
           }
         } else {
 #pragma unroll
-          for (int j = 0; j < NP; ++j)
-#pragma unroll
-            for (int q = 0; q < 9; ++q) acc[j][q] = fmaf(w[j], v[q], acc[j][q]);
+          for (int j = 0; j < NP; ++j) {
+            const float2 ww = make_float2(w[j], w[j]);
+            float2* A = acc[j];
+            A[0] = __ffma2_rn(ww, make_float2(v[0], v[1]), A[0]);
+            A[1] = __ffma2_rn(ww, make_float2(v[2], v[3]), A[1]);
+            A[2] = __ffma2_rn(ww, make_float2(v[4], v[5]), A[2]);
+            A[3] = __ffma2_rn(ww, make_float2(v[6], v[7]), A[3]);
+            A[4].x = fmaf(w[j], v[8], A[4].x);
+          }
         }
       }
     }
@@ -634,7 +647,9 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
     int taken = -1;
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
-      const float* A = acc[j];
+      float A[NA];
+#pragma unroll
+      for (int a = 0; a < NA; ++a) A[a] = (a & 1) ? acc[j][a / 2].y : acc[j][a / 2].x;
       const float s0 = A[0], s1 = A[1];
       const float enl = s0 * s0 / s1;
       float alpha = 0.0f;
@@ -673,7 +688,7 @@ __device__ __forceinline__ void fast3_pass(const FilterParams& P, const PassPara
     for (int j = 0; j < NP; ++j)
       if (taken == j) {
 #pragma unroll
-        for (int q = 0; q < 9; ++q) best.m[q] = acc[j][q];
+        for (int q = 0; q < 9; ++q) best.m[q] = (q & 1) ? acc[j][q / 2].y : acc[j][q / 2].x;
       }
   }
 }
